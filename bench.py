@@ -1,0 +1,363 @@
+"""Benchmark of the big-integer multiply path (one JSON line on rank 0).
+
+Workload: BASELINE configuration 2 -- one plain 2^28-bit x 2^28-bit product
+(2^23 u32 words each, uniform random with the top bit set, seeded), 32-bit
+coefficients, n = 2^24, two 62-bit primes (64-bit prime path).  A "step" is
+one full product.  Metric: products/s (whole job), with the per-stage times,
+the HBM roofline of the dominant kernel and the product-level algorithmic
+byte model (12*K*n*w + in + out) beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config 1|2|2sq]
+
+Multi-GPU: products are independent, so N ranks run N replicas (no
+collective on the data path, "scaling": "weak"); the timed region is
+bracketed by a barrier and the max over ranks is reported.
+
+--impl reference times the CPU restatement of the reference's algorithm
+(oracle/, the reference has no CPU multiply of its own and its GPU NTT
+library is absent) on this host's cores, on the same configuration.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_HBM_GBS = 6650.0
+
+CONFIGS = {
+    # name: (words_a, words_b, path, K, square, description)
+    "2": (1 << 23, 1 << 23, 64, 2, False,
+          "plain 2^28-bit x 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
+    "2sq": (1 << 23, 1 << 23, 64, 2, True,
+            "squaring 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
+    "1": (1 << 15, 1 << 15, 32, 3, False,
+          "plain 2^20-bit x 2^20-bit, 16-bit coefficients, n=2^17, 3 x 30-bit primes"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+def operands(cfg, rank):
+    from oracle import mt64
+    la, lb, path, K, square, _ = CONFIGS[cfg]
+    a = mt64.random_words_top_fast(la, 1234 + 1000 * rank)
+    b = a if square else mt64.random_words_top_fast(lb, 5678 + 1000 * rank)
+    return a, b
+
+
+def model_bytes(la, lb, n, K, w, square):
+    """Per-kernel split of the fixed algorithmic byte model
+    12*K*n*w + in + out (9*K*n*w + in + out when squaring)."""
+    knw = K * n * w
+    ops = 1 if square else 2
+    fwd = 4 * (la + (0 if square else lb)) + ops * knw          # FWD pass 1 (A, B)
+    row = ops * 2 * knw + 3 * knw                               # FWD pass 2 + INV pass 1
+    inv = 2 * knw                                               # INV pass 2
+    carry = knw + 4 * (la + lb)                                 # Garner + carry
+    return {"fwd_ms": fwd, "mul_ms": row, "intt_ms": inv, "crt_carry_ms": carry}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_traffic(cfg, kernel):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)[cfg][kernel]
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_baseline(cfg, budget_s=20.0):
+    """The oracle (CPU restatement of the reference's algorithm) with all host
+    threads on the same operands: full products until the budget is spent
+    (at least one).  GMP mpz_mul (single thread) is reported beside it."""
+    from oracle import gmp_ref, oracle
+    la, lb, path, K, square, _ = CONFIGS[cfg]
+    a, b = operands(cfg, 0)
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    n_done, t0 = 0, time.perf_counter()
+    while True:
+        oracle.multiply(a, b, path, K)
+        n_done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    g = gmp_ref.time_mul(a, b, 1)
+    return {"value": n_done / dt, "unit": "products/s", "cores": cores, "kind": "port",
+            "sample": f"{n_done} full product(s) of the workload, oracle/bw_oracle.c on "
+                      f"{cores} threads, {dt:.1f} s",
+            "gmp": {"value": 1.0 / g, "unit": "products/s", "cores": 1,
+                    "impl": f"GMP {gmp_ref.version} mpz_mul, single thread"}}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    la, lb, path, K, square, desc = CONFIGS[args.config]
+    a, b = operands(args.config, 0)
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    t0 = time.perf_counter()
+    oracle.multiply(a, b, path, K)
+    t_one = time.perf_counter() - t0
+    # bounded: at most ~150 s of timed work whatever --steps asks for
+    steps = max(1, min(args.steps, int(150.0 / max(t_one, 1e-3))))
+    warm = min(args.warmup, 1)
+    for _ in range(warm):
+        oracle.multiply(a, b, path, K)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.multiply(a, b, path, K)
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    line = {
+        "impl": "reference", "metric": "products/s", "value": v, "unit": "products/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1000 * dt / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic", "config": {"workload": f"config {args.config}: {desc}",
+                                        "words_a": la, "words_b": lb, "path": path,
+                                        "num_primes": K},
+        "cpu_baseline": {"value": v, "unit": "products/s", "cores": cores, "kind": "port",
+                         "sample": f"{steps} full products (requested {args.steps}), "
+                                   f"oracle/bw_oracle.c on {cores} threads"},
+        "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference's GPU pipeline needs the absent GPU-NTT library; this is the "
+                "CPU restatement of its algorithm (radix-2 NTT, Garner, carry)",
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import birdwing_b200 as bw
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    la, lb, path, K, square, desc = CONFIGS[args.config]
+    a, b = operands(args.config, rank)
+    plan = bw.Plan(la, lb, path, K)
+    ctx = bw.Context(plan)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = plan.N
+    w = 8 if path == 64 else 4
+
+    # inputs resident in HBM for the device-time measurement
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = da if square else torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.empty(la + lb, dtype=torch.int32, device="cuda")
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+
+    def step(timing):
+        return ctx.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, dc.data_ptr(), la + lb,
+                                   timing=timing)
+
+    for _ in range(max(3, args.warmup)):
+        step(False)
+    ctx.sync()
+    # correctness of the benchmarked product (once, outside the timed region)
+    if rank == 0:
+        from oracle import gmp_ref
+        got = dc.cpu().numpy().view(np.uint32)
+        ok = bool((got == gmp_ref.mul(a, b)).all())
+    else:
+        ok = True
+
+    sampler = ClockSampler(local)
+    stage = {k: [] for k in ("fwd_ms", "mul_ms", "intt_ms", "crt_carry_ms")}
+    per_step = []
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i)                       # evict L2 between steps
+            ev0[i].record(stream)
+        t = step(True)                           # synchronises on its last event
+        with torch.cuda.stream(stream):
+            ev1[i].record(stream)
+        for k in stage:
+            stage[k].append(t[k])
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ctx.sync()
+    for i in range(args.steps):
+        per_step.append(ev0[i].elapsed_time(ev1[i]))
+    total_ms = sum(per_step)
+    t_max = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    total_ms = float(t_max.item())
+
+    # end to end through the C ABI with pinned host buffers
+    ha = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    hb = ha if square else torch.from_numpy(b.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    hc = torch.empty(la + lb, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    for _ in range(2):
+        ctx.multiply(ha, hb, out=hc)
+    barrier()
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        ctx.multiply(ha, hb, out=hc)
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_total = float(e2e_t.item())
+
+    if rank == 0:
+        ms = total_ms / args.steps
+        mb = model_bytes(la, lb, n, K, w, square)
+        means = {k: statistics.mean(v) for k, v in stage.items()}
+        dom = max(means, key=means.get)
+        kernel_names = {"fwd_ms": "k_fwd_col", "mul_ms": "k_row", "intt_ms": "k_inv_col",
+                        "crt_carry_ms": "k_garner_carry"}
+        peak, peak_kind = load_peaks()
+        achieved = mb[dom] / (means[dom] * 1e-3) / 1e9
+        total_model = sum(mb.values())
+        line = {
+            "metric": "products/s", "value": world * args.steps / (total_ms * 1e-3),
+            "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64" if path == 64 else "u32", "data": "synthetic",
+            "config": {"workload": f"config {args.config}: {desc}", "words_a": la,
+                       "words_b": lb, "path": path, "num_primes": K, "log_n": plan.logN,
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "correct_vs_gmp": ok,
+            "stage_ms": means,
+            "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind,
+                         "traffic": load_traffic(args.config, kernel_names[dom]),
+                         "algorithmic_bytes": mb[dom]},
+            "product_roofline": {"model_bytes": total_model,
+                                 "achieved": total_model / (ms * 1e-3) / 1e9, "unit": "GB/s",
+                                 "frac": total_model / (ms * 1e-3) / 1e9 / peak},
+            "e2e": {"value": world * args.e2e_steps / (e2e_total * 1e-3),
+                    "unit": "products/s", "h2d_bytes_per_step": 4 * (la + (0 if square else lb)),
+                    "d2h_bytes_per_step": 4 * (la + lb) + 4},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.config)
+        print(json.dumps(line))
+    ctx.close()
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

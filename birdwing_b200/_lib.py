@@ -1,0 +1,118 @@
+"""ctypes binding of libbirdwing.so (the C ABI declared in include/birdwing.h).
+
+Importing this module loads the in-tree shared library.  There is no
+fallback: if the library is missing the import fails with a message that
+says how to build it.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbirdwing.so")
+
+BW_OK = 0
+BW_EINVAL = -1
+BW_ENOMEM = -2
+BW_ECUDA = -3
+BW_ETIMEOUT = -4
+BW_EREJECT = -5
+BW_ESIZE = -6
+BW_ECHECK = -7
+BW_EBUSY = -8
+
+BW_PATH_AUTO = 0
+BW_PATH_P32 = 32
+BW_PATH_P64 = 64
+
+BW_PTR_HOST = 0
+BW_PTR_DEVICE = 1
+
+_NAMES = {
+    BW_EINVAL: "BW_EINVAL", BW_ENOMEM: "BW_ENOMEM", BW_ECUDA: "BW_ECUDA",
+    BW_ETIMEOUT: "BW_ETIMEOUT", BW_EREJECT: "BW_EREJECT", BW_ESIZE: "BW_ESIZE",
+    BW_ECHECK: "BW_ECHECK", BW_EBUSY: "BW_EBUSY",
+}
+
+
+class BwError(RuntimeError):
+    """A negative status from the C ABI, with bw_last_error()'s message."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class bw_timing(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in
+                ("h2d_ms", "fwd_ms", "mul_ms", "intt_ms", "crt_carry_ms", "d2h_ms", "total_ms")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class bw_plan_info(ctypes.Structure):
+    _fields_ = [
+        ("path", ctypes.c_int), ("num_primes", ctypes.c_int), ("log_n", ctypes.c_int),
+        ("log_rows", ctypes.c_int), ("log_cols", ctypes.c_int), ("coeff_bits", ctypes.c_int),
+        ("la", ctypes.c_size_t), ("lb", ctypes.c_size_t), ("lc", ctypes.c_size_t),
+        ("plan_device_bytes", ctypes.c_size_t), ("ctx_device_bytes", ctypes.c_size_t),
+        ("primes", ctypes.c_uint64 * 3),
+    ]
+
+
+class bw_limits_info(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("num_primes", ctypes.c_int),
+                ("max_log_n", ctypes.c_int), ("max_square_words", ctypes.c_size_t)]
+
+
+# symbol -> (restype, argtypes)
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_I = ctypes.c_int
+_U = ctypes.c_uint
+SIGNATURES = {
+    "bw_abi_version": (_I, []),
+    "bw_last_error": (ctypes.c_char_p, []),
+    "bw_limits": (_I, [_I, _I, ctypes.POINTER(bw_limits_info)]),
+    "bw_size_supported": (_I, [_I, _I, _SZ, _SZ]),
+    "bw_plan_create": (_I, [ctypes.POINTER(_P), _I, _SZ, _SZ, _I, _U]),
+    "bw_plan_destroy": (_I, [_P]),
+    "bw_plan_get_info": (_I, [_P, ctypes.POINTER(bw_plan_info)]),
+    "bw_ctx_create": (_I, [ctypes.POINTER(_P), _P, _P]),
+    "bw_ctx_destroy": (_I, [_P]),
+    "bw_ctx_stream": (_P, [_P]),
+    "bw_ctx_sync": (_I, [_P]),
+    "bw_multiply": (_I, [_P, _P, _SZ, _P, _SZ, _P, _SZ, _U, ctypes.POINTER(bw_timing)]),
+    "bw_square": (_I, [_P, _P, _SZ, _P, _SZ, _U, ctypes.POINTER(bw_timing)]),
+    "bw_multiply_coeffs": (_I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
+    "bw_ctx_set_wait_limit": (_I, [_P, _I]),
+    "bw_ctx_inject_wait_fault": (_I, [_P, _I]),
+    "bw_multiply_host_once": (_I, [_P, _SZ, _P, _SZ, _P, _SZ, _I,
+                                   ctypes.POINTER(ctypes.c_float)]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python birdwing_b200/build.py` "
+            "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error():
+    return lib.bw_last_error().decode(errors="replace")
+
+
+def check(rc):
+    if rc != BW_OK:
+        raise BwError(rc, last_error())
+    return rc

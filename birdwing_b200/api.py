@@ -1,0 +1,226 @@
+"""Python mirror of the reference's host API for the multiply path.
+
+Names follow the reference (nikitaborisov/birdwing):
+
+  * ``host_multiply_merge(A, B)``   -- include/multiply.h:9-23, one-shot product
+  * ``Plan``   ~ NTTPrecomputed      -- precompute_ntt + upload_ntt_precomputed
+  * ``Context`` ~ NTTContext          -- allocate_ntt_context
+  * ``Context.execute``               -- execute_ntt_multiply (incl. the CRT dump)
+
+Operands are little-endian arrays of 32-bit words (numpy uint32); a u64 limb
+array (the reference's NATIVE_HOST_LIMBS pipeline) is the same memory viewed
+as twice as many u32 words.  Every call goes through libbirdwing.so; errors
+raise BwError (the reference prints and calls exit(1) instead,
+src/ntt_limits.cpp:256-280).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import BwError, check, lib
+
+__all__ = [
+    "Plan", "Context", "host_multiply_merge", "host_multiply_merge_native", "multiply",
+    "square", "limits", "size_supported", "int_to_limbs", "limbs_to_int", "BwError",
+]
+
+
+def int_to_limbs(x, n=None):
+    """Python int -> little-endian uint32 array (of length n if given)."""
+    if x < 0:
+        raise ValueError("negative")
+    nbytes = max(1, (x.bit_length() + 7) // 8)
+    if n is not None:
+        nbytes = max(nbytes, 4 * n)
+    nbytes = (nbytes + 3) // 4 * 4
+    a = np.frombuffer(x.to_bytes(nbytes, "little"), dtype="<u4").copy()
+    if n is not None:
+        if np.any(a[n:]):
+            raise ValueError("value does not fit in n words")
+        a = a[:n]
+    return a
+
+
+def limbs_to_int(a):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint64:
+        a = a.view(np.uint32)
+    return int.from_bytes(np.ascontiguousarray(a, dtype="<u4").tobytes(), "little")
+
+
+def _as_u32(a):
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint64:
+        return a.view(np.uint32)
+    if a.dtype != np.uint32:
+        raise TypeError(f"limbs must be uint32 or uint64, got {a.dtype}")
+    return a
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def limits(path=L.BW_PATH_P64, num_primes=0):
+    info = L.bw_limits_info()
+    check(lib.bw_limits(path, num_primes, ctypes.byref(info)))
+    return {"path": info.path, "num_primes": info.num_primes, "max_log_n": info.max_log_n,
+            "max_square_words": info.max_square_words}
+
+
+def size_supported(la, lb, path=L.BW_PATH_AUTO, num_primes=0):
+    """(ok, why) -- reference: multiply_size_supported(L_A, L_B, &why)."""
+    rc = lib.bw_size_supported(path, num_primes, la, lb)
+    return rc == L.BW_OK, ("" if rc == L.BW_OK else L.last_error())
+
+
+class Plan:
+    """Per-size tables on the device (twiddles, Garner constants)."""
+
+    def __init__(self, la, lb, path=L.BW_PATH_AUTO, num_primes=0):
+        h = ctypes.c_void_p()
+        check(lib.bw_plan_create(ctypes.byref(h), path, la, lb, num_primes, 0))
+        self._h = h
+        info = L.bw_plan_info()
+        check(lib.bw_plan_get_info(self._h, ctypes.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in L.bw_plan_info._fields_ if f != "primes"}
+        self.info["primes"] = [int(p) for p in info.primes[: info.num_primes]]
+        self.la, self.lb = la, lb
+        self.N = 1 << info.log_n
+        self.logN = info.log_n
+
+    def close(self):
+        if self._h:
+            lib.bw_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Context:
+    """Device scratch + stream for products of one plan's size."""
+
+    def __init__(self, plan, stream=None):
+        h = ctypes.c_void_p()
+        check(lib.bw_ctx_create(ctypes.byref(h), plan._h, ctypes.c_void_p(stream or 0)))
+        self._h = h
+        self.plan = plan
+
+    @property
+    def stream(self):
+        return lib.bw_ctx_stream(self._h)
+
+    def close(self):
+        if self._h:
+            lib.bw_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def multiply(self, a, b, out=None, timing=False):
+        """Host arrays in, host array out (copies and synchronises)."""
+        a = _as_u32(a)
+        b = _as_u32(b)
+        lc = a.size + b.size
+        if out is None:
+            out = np.empty(lc, dtype=np.uint32)
+        t = L.bw_timing()
+        same = a is b
+        check(lib.bw_multiply(self._h, _ptr(a), a.size, _ptr(a) if same else _ptr(b), b.size,
+                              _ptr(out), out.size, L.BW_PTR_HOST,
+                              ctypes.byref(t) if timing else None))
+        return (out, t.as_dict()) if timing else out
+
+    def square(self, a, out=None, timing=False):
+        a = _as_u32(a)
+        if out is None:
+            out = np.empty(2 * a.size, dtype=np.uint32)
+        t = L.bw_timing()
+        check(lib.bw_square(self._h, _ptr(a), a.size, _ptr(out), out.size, L.BW_PTR_HOST,
+                            ctypes.byref(t) if timing else None))
+        return (out, t.as_dict()) if timing else out
+
+    def multiply_device(self, a_ptr, la, b_ptr, lb, c_ptr, lc, timing=False):
+        """Device pointers (ints); enqueues on the context stream."""
+        t = L.bw_timing()
+        check(lib.bw_multiply(self._h, ctypes.c_void_p(a_ptr), la, ctypes.c_void_p(b_ptr), lb,
+                              ctypes.c_void_p(c_ptr), lc, L.BW_PTR_DEVICE,
+                              ctypes.byref(t) if timing else None))
+        return t.as_dict() if timing else None
+
+    def sync(self):
+        check(lib.bw_ctx_sync(self._h))
+
+    def coeffs(self, a, b):
+        """Convolution coefficients after Garner, as Python ints (length n)."""
+        a = _as_u32(a)
+        b = _as_u32(b)
+        n = self.plan.N
+        w = np.empty(3 * n, dtype=np.uint32)
+        same = a is b
+        check(lib.bw_multiply_coeffs(self._h, _ptr(a), a.size, _ptr(a) if same else _ptr(b),
+                                     b.size, _ptr(w), w.size))
+        w = w.reshape(n, 3).astype(object)
+        return [int(r[0]) | (int(r[1]) << 32) | (int(r[2]) << 64) for r in w]
+
+    # reference spelling: execute_ntt_multiply(ctx, a, b, C_out, timing)
+    def execute(self, a, b, timing=False):
+        return self.multiply(a, b, timing=timing)
+
+
+def multiply(a, b, path=L.BW_PATH_AUTO):
+    """One-shot product of two uint32 arrays (plan, context, multiply, teardown)."""
+    a = _as_u32(a)
+    b = _as_u32(b)
+    out = np.empty(a.size + b.size, dtype=np.uint32)
+    ms = ctypes.c_float()
+    check(lib.bw_multiply_host_once(_ptr(a), a.size, _ptr(b), b.size, _ptr(out), out.size, path,
+                                    ctypes.byref(ms)))
+    return out
+
+
+def square(a, path=L.BW_PATH_AUTO):
+    with Plan(len(a), len(a), path) as p, Context(p) as c:
+        return c.square(a)
+
+
+def host_multiply_merge(A, B):
+    """Reference: host_multiply_merge (src/host_multiply.cpp:27-86).  Returns
+    (C, duration_ms) with C of length len(A) + len(B)."""
+    A = np.asarray(A, dtype=np.uint32)
+    B = np.asarray(B, dtype=np.uint32)
+    out = np.empty(A.size + B.size, dtype=np.uint32)
+    ms = ctypes.c_float()
+    check(lib.bw_multiply_host_once(_ptr(A), A.size, _ptr(B), B.size, _ptr(out), out.size,
+                                    L.BW_PATH_AUTO, ctypes.byref(ms)))
+    return out, ms.value
+
+
+def host_multiply_merge_native(A, B):
+    """Reference: host_multiply_merge_native (src/host_multiply.cpp:90-134):
+    u64 limbs in, u64 limbs out."""
+    A = np.ascontiguousarray(A, dtype=np.uint64)
+    B = np.ascontiguousarray(B, dtype=np.uint64)
+    out, ms = host_multiply_merge(A.view(np.uint32), B.view(np.uint32))
+    return out.view(np.uint64), ms

@@ -1,0 +1,761 @@
+// bw_core.cu -- plans, contexts, kernel launches and the C ABI (birdwing.h).
+//
+// Lifecycle (reference: precompute_ntt / upload_ntt_precomputed /
+// allocate_ntt_context / execute_ntt_multiply / cleanup_*,
+// src/gpu_ntt.cu:240-1018, and the five timing buckets of docs/TIMING.md):
+//   bw_plan_create  = precompute + upload: O(R + C + sqrt(n)) twiddles per
+//                     prime, built on the host and copied once;
+//   bw_ctx_create   = allocate: residue scratch, staging, carry state, stream;
+//   bw_multiply     = execute: H2D (host mode), K1..K4 on one stream, D2H;
+//   *_destroy       = cleanup.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/birdwing.h"
+#include "bw_host.h"
+#include "bw_kernels.cuh"
+
+using namespace bw;
+
+// ------------------------------------------------------------------ errors
+
+static thread_local std::string g_last_error;
+
+int bw_fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+void bw_clear_error() { g_last_error.clear(); }
+
+#define BW_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            return bw_fail(e_ == cudaErrorMemoryAllocation ? BW_ENOMEM : BW_ECUDA,      \
+                           "%s failed: %s", #call, cudaGetErrorString(e_));             \
+        }                                                                               \
+    } while (0)
+
+// ------------------------------------------------------------------ host math
+
+namespace {
+
+using u128 = unsigned __int128;
+
+uint64_t mulmod(uint64_t a, uint64_t b, uint64_t p) { return (uint64_t)((u128)a * b % p); }
+uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
+    uint64_t r = 1 % p;
+    a %= p;
+    while (e) {
+        if (e & 1) r = mulmod(r, a, p);
+        a = mulmod(a, a, p);
+        e >>= 1;
+    }
+    return r;
+}
+uint64_t invmod(uint64_t a, uint64_t p) { return powmod(a % p, p - 2, p); }
+uint64_t shoup_pre(uint64_t w, uint64_t p, int bits) {
+    return bits == 64 ? (uint64_t)(((u128)w << 64) / p) : (uint64_t)((((uint64_t)w) << 32) / p);
+}
+uint64_t neg_inv_pow2(uint64_t p, int bits) {
+    uint64_t x = 1;  // Newton: x = x * (2 - p x) doubles the correct bits
+    for (int i = 0; i < 7; ++i) x *= 2 - p * x;
+    if (bits == 32) x &= 0xffffffffull;
+    const uint64_t m = bits == 64 ? ~0ull : 0xffffffffull;
+    return (0 - x) & m;
+}
+uint32_t bitrev_h(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; ++i) {
+        r = (r << 1) | (x & 1);
+        x >>= 1;
+    }
+    return r;
+}
+
+// Primes of the two paths with a generator of the multiplicative group.
+// P64: c * 2^32 + 1 just below 2^62 (v2(p-1) = 33, 34, 37).
+// P32: 30-bit primes with v2(p-1) = 24, 26, 25.
+const uint64_t kP64[3] = {0x3fffffee00000001ull, 0x3fffffb400000001ull, 0x3fffffa000000001ull};
+const uint64_t kG64[3] = {3, 19, 3};
+const uint64_t kP32[3] = {754974721ull, 469762049ull, 167772161ull};
+const uint64_t kG32[3] = {11, 3, 3};
+
+int v2(uint64_t x) {
+    int k = 0;
+    while ((x & 1) == 0) {
+        x >>= 1;
+        ++k;
+    }
+    return k;
+}
+
+}  // namespace
+
+int bw_path_max_log_n(int path, int K) {
+    const uint64_t* P = path == BW_PATH_P64 ? kP64 : kP32;
+    int m = 64;
+    for (int k = 0; k < K; ++k) m = std::min(m, v2(P[k] - 1));
+    const int design = path == BW_PATH_P64 ? 26 : 26;  // two-level 4-step limit
+    return std::min(m, design);
+}
+
+const uint64_t* bw_path_primes(int path) { return path == BW_PATH_P64 ? kP64 : kP32; }
+
+// ------------------------------------------------------------------ plan
+
+struct bw_plan {
+    int path = 0, K = 0;
+    size_t la = 0, lb = 0, nca = 0, ncb = 0;
+    int log_n = 0, log_r = 0, log_c = 0, log_cb = 0, lo = 0;
+    int device = 0;
+    bool zt_a = false, zt_b = false;
+    void* d_tables = nullptr;
+    size_t table_bytes = 0;
+    PlanDev<Ar32> pd32{};
+    PlanDev<Ar64> pd64{};
+    uint64_t primes[3] = {0, 0, 0};
+};
+
+namespace {
+
+template <class Ar>
+struct TableBuilder {
+    using T = typename Ar::T;
+    std::vector<Tw<T>> host;
+    // returns element offset of a new table
+    size_t add_stage_table(uint64_t p, uint64_t root, int log_len, int bits) {
+        const size_t L = (size_t)1 << log_len;
+        const size_t off = host.size();
+        host.resize(off + std::max<size_t>(L, 1));
+        std::vector<uint64_t> pw(std::max<size_t>(L / 2, 1));
+        pw[0] = 1;
+        for (size_t j = 1; j < pw.size(); ++j) pw[j] = mulmod(pw[j - 1], root, p);
+        host[off] = Tw<T>{0, 0};
+        for (int s = 0; s < log_len; ++s) {
+            const size_t m = (size_t)1 << s;
+            for (size_t i = 0; i < m; ++i) {
+                const size_t e = (L >> (s + 1)) * bitrev_h((uint32_t)i, s);
+                const uint64_t w = pw[e];
+                host[off + m + i] = Tw<T>{(T)w, (T)shoup_pre(w, p, bits)};
+            }
+        }
+        return off;
+    }
+    size_t add_power_table(uint64_t p, uint64_t base, size_t count, uint64_t scale, int bits) {
+        const size_t off = host.size();
+        host.resize(off + count);
+        uint64_t w = scale % p;
+        for (size_t j = 0; j < count; ++j) {
+            host[off + j] = Tw<T>{(T)w, (T)shoup_pre(w, p, bits)};
+            w = mulmod(w, base, p);
+        }
+        return off;
+    }
+};
+
+template <class Ar>
+int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
+    using T = typename Ar::T;
+    const int bits = Ar::BITS;
+    const uint64_t* P = pl->path == BW_PATH_P64 ? kP64 : kP32;
+    const uint64_t* Gn = pl->path == BW_PATH_P64 ? kG64 : kG32;
+    TableBuilder<Ar> tb;
+    size_t off[kMaxPrimes][8];
+    const size_t n = (size_t)1 << pl->log_n;
+    for (int k = 0; k < pl->K; ++k) {
+        const uint64_t p = P[k];
+        const uint64_t wn = powmod(Gn[k], (p - 1) >> pl->log_n, p);  // primitive n-th root
+        const uint64_t wni = invmod(wn, p);
+        const uint64_t wr = powmod(wn, (uint64_t)1 << pl->log_c, p);  // R-th root
+        const uint64_t wc = powmod(wn, (uint64_t)1 << pl->log_r, p);  // C-th root
+        off[k][0] = tb.add_stage_table(p, wr, pl->log_r, bits);
+        off[k][1] = tb.add_stage_table(p, invmod(wr, p), pl->log_r, bits);
+        off[k][2] = tb.add_stage_table(p, wc, pl->log_c, bits);
+        off[k][3] = tb.add_stage_table(p, invmod(wc, p), pl->log_c, bits);
+        const size_t nlo = (size_t)1 << pl->lo, nhi = n >> pl->lo;
+        const uint64_t scale = mulmod(invmod(n % p, p), powmod(2, bits, p), p);
+        off[k][4] = tb.add_power_table(p, wn, nlo, 1, bits);
+        off[k][5] = tb.add_power_table(p, powmod(wn, nlo, p), nhi, 1, bits);
+        off[k][6] = tb.add_power_table(p, wni, nlo, 1, bits);
+        off[k][7] = tb.add_power_table(p, powmod(wni, nlo, p), nhi, scale, bits);
+    }
+    pl->table_bytes = tb.host.size() * sizeof(Tw<T>);
+    BW_CUDA(cudaMalloc(&pl->d_tables, pl->table_bytes));
+    BW_CUDA(cudaMemcpy(pl->d_tables, tb.host.data(), pl->table_bytes, cudaMemcpyHostToDevice));
+    const Tw<T>* base = reinterpret_cast<const Tw<T>*>(pl->d_tables);
+    for (int k = 0; k < pl->K; ++k) {
+        auto& pr = pd.pr[k];
+        pr.WRf = base + off[k][0];
+        pr.WRi = base + off[k][1];
+        pr.WCf = base + off[k][2];
+        pr.WCi = base + off[k][3];
+        pr.TLf = base + off[k][4];
+        pr.THf = base + off[k][5];
+        pr.TLi = base + off[k][6];
+        pr.THi = base + off[k][7];
+        pr.ar.p = (T)P[k];
+        pr.ar.p2 = (T)(2 * P[k]);
+        pr.ar.pinv = (T)neg_inv_pow2(P[k], bits);
+        pr.one_q = (T)shoup_pre(1, P[k], bits);
+    }
+    // unused prime slots get harmless arithmetic constants
+    for (int k = pl->K; k < kMaxPrimes; ++k) pd.pr[k] = pd.pr[0];
+    auto& g = pd.gar;
+    const uint64_t p0 = P[0], p1 = P[1], p2 = P[2];
+    g.p0 = p0;
+    g.inv1 = (T)invmod(p0 % p1, p1);
+    g.inv1q = (T)shoup_pre(g.inv1, p1, bits);
+    g.p0m2 = (T)(p0 % p2);
+    g.p0m2q = (T)shoup_pre(g.p0m2, p2, bits);
+    g.inv2 = (T)invmod(mulmod(p0 % p2, p1 % p2, p2), p2);
+    g.inv2q = (T)shoup_pre(g.inv2, p2, bits);
+    pd.K = pl->K;
+    pd.log_n = pl->log_n;
+    pd.log_r = pl->log_r;
+    pd.log_c = pl->log_c;
+    pd.lo = pl->lo;
+    pd.log_cb = pl->log_cb;
+    return BW_OK;
+}
+
+int ceil_log2(size_t x) {
+    int k = 0;
+    while (((size_t)1 << k) < x) ++k;
+    return k;
+}
+
+}  // namespace
+
+int bw_check_size(int path, int K, size_t la, size_t lb, int* log_n_out) {
+    if (path != BW_PATH_P32 && path != BW_PATH_P64)
+        return bw_fail(BW_EINVAL, "unknown path %d", path);
+    if (K < 2 || K > 3) return bw_fail(BW_EINVAL, "num_primes must be 2 or 3 (got %d)", K);
+    if (la == 0 || lb == 0) return bw_fail(BW_ESIZE, "operand limb count must be positive");
+    const int cpw = path == BW_PATH_P32 ? 2 : 1;
+    const size_t nca = la * cpw, ncb = lb * cpw;
+    // n >= 16 keeps every 64-byte vector load of the Garner kernel in bounds
+    const int log_n = std::max(4, ceil_log2(nca + ncb - 1));
+    const int max_log = bw_path_max_log_n(path, K);
+    if (log_n > max_log)
+        return bw_fail(BW_ESIZE,
+                       "transform length 2^%d for %zu x %zu words exceeds the %d-bit path limit "
+                       "2^%d",
+                       log_n, la, lb, path, max_log);
+    // CRT bound: min(L_A, L_B) * (2^b - 1)^2 < p0 * p1 (the reference's bound,
+    // src/ntt_limits.cpp:82-95, against the first two primes: a third prime is
+    // kept redundant so that it can check the reconstruction)
+    const uint64_t* P = bw_path_primes(path);
+    const int cb = path == BW_PATH_P32 ? 16 : 32;
+    const long double lim = (long double)P[0] * (long double)P[1];
+    const long double cmax = (long double)std::min(nca, ncb) * powl(2.0L, 2 * cb);
+    if (!(cmax < lim))
+        return bw_fail(BW_ESIZE, "convolution coefficient bound exceeds the CRT modulus product");
+    if (log_n_out) *log_n_out = log_n;
+    return BW_OK;
+}
+
+static int choose_path(size_t la, size_t lb) {
+    (void)la;
+    (void)lb;
+    return BW_PATH_P64;
+}
+
+extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int num_primes,
+                              unsigned flags) {
+    (void)flags;
+    bw_clear_error();
+    if (!out) return bw_fail(BW_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (path == BW_PATH_AUTO) path = choose_path(la, lb);
+    const int K = num_primes == 0 ? 2 : num_primes;
+    int log_n = 0;
+    int rc = bw_check_size(path, K, la, lb, &log_n);
+    if (rc) return rc;
+    bw_plan* pl = new bw_plan();
+    pl->path = path;
+    pl->K = K;
+    pl->la = la;
+    pl->lb = lb;
+    const int cpw = path == BW_PATH_P32 ? 2 : 1;
+    pl->nca = la * cpw;
+    pl->ncb = lb * cpw;
+    pl->log_n = log_n;
+    const int w = path == BW_PATH_P64 ? 8 : 4;
+    const int max_c = path == BW_PATH_P64 ? 13 : 14;
+    pl->log_c = std::min(max_c, (log_n + 1) / 2);
+    pl->log_r = log_n - pl->log_c;
+    // column tile: 64 KiB of residues per shared-memory buffer
+    int log_cb = 0;
+    while (log_cb < pl->log_c && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536) ++log_cb;
+    pl->log_cb = log_cb;
+    pl->lo = (log_n + 1) / 2;
+    const size_t half = ((size_t)1 << log_n) / 2;
+    pl->zt_a = pl->nca <= half;
+    pl->zt_b = pl->ncb <= half;
+    for (int k = 0; k < K; ++k) pl->primes[k] = bw_path_primes(path)[k];
+    cudaGetDevice(&pl->device);
+    rc = path == BW_PATH_P64 ? build_tables<Ar64>(pl, pl->pd64) : build_tables<Ar32>(pl, pl->pd32);
+    if (rc) {
+        if (pl->d_tables) cudaFree(pl->d_tables);
+        delete pl;
+        return rc;
+    }
+    *out = pl;
+    return BW_OK;
+}
+
+extern "C" int bw_plan_destroy(bw_plan* pl) {
+    if (!pl) return BW_OK;
+    if (pl->d_tables) cudaFree(pl->d_tables);
+    delete pl;
+    return BW_OK;
+}
+
+static size_t ctx_bytes(const bw_plan* pl) {
+    const size_t n = (size_t)1 << pl->log_n;
+    const int w = pl->path == BW_PATH_P64 ? 8 : 4;
+    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
+    const size_t nl = n / cpw;
+    const size_t ntiles = (nl + kCarryTileWords - 1) / kCarryTileWords;
+    return 2 * (size_t)pl->K * n * w + (pl->la + pl->lb) * 4 * 2 + 64 + ntiles * 20;
+}
+
+extern "C" int bw_plan_get_info(const bw_plan* pl, bw_plan_info* o) {
+    if (!pl || !o) return bw_fail(BW_EINVAL, "NULL argument");
+    memset(o, 0, sizeof *o);
+    o->path = pl->path;
+    o->num_primes = pl->K;
+    o->log_n = pl->log_n;
+    o->log_rows = pl->log_r;
+    o->log_cols = pl->log_c;
+    o->coeff_bits = pl->path == BW_PATH_P32 ? 16 : 32;
+    o->la = pl->la;
+    o->lb = pl->lb;
+    o->lc = pl->la + pl->lb;
+    o->plan_device_bytes = pl->table_bytes;
+    o->ctx_device_bytes = ctx_bytes(pl);
+    for (int k = 0; k < 3; ++k) o->primes[k] = k < pl->K ? pl->primes[k] : 0;
+    return BW_OK;
+}
+
+// ------------------------------------------------------------------ context
+
+struct bw_ctx {
+    const bw_plan* plan = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    void* d_res_a = nullptr;
+    void* d_res_b = nullptr;
+    uint32_t* d_in = nullptr;   // staging: a then b
+    uint32_t* d_out = nullptr;  // staging: product
+    unsigned char* d_state = nullptr;
+    size_t state_bytes = 0;
+    CarryState* cst = nullptr;
+    uint32_t* err = nullptr;
+    uint4* rec_x = nullptr;
+    uint32_t* rec_s = nullptr;
+    size_t ntiles = 0;
+    uint32_t epoch = 0;
+    uint32_t* h_err = nullptr;  // pinned
+    cudaEvent_t ev[8] = {};
+    int spin_limit = 1 << 22;
+    bool inject_wait_fault = false;
+};
+
+extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
+    bw_clear_error();
+    if (!out || !pl) return bw_fail(BW_EINVAL, "NULL argument");
+    *out = nullptr;
+    bw_ctx* c = new bw_ctx();
+    c->plan = pl;
+    auto fail = [&](int rc) {
+        bw_ctx_destroy(c);
+        return rc;
+    };
+    const size_t n = (size_t)1 << pl->log_n;
+    const int w = pl->path == BW_PATH_P64 ? 8 : 4;
+    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
+    const size_t res_bytes = (size_t)pl->K * n * w;
+    cudaError_t e;
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(bw_fail(BW_ECUDA, "stream: %s", cudaGetErrorString(e)));
+        c->own_stream = true;
+    }
+    if ((e = cudaMalloc(&c->d_res_a, res_bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&c->d_res_b, res_bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&c->d_in, ((pl->la + pl->lb + 3) & ~(size_t)3) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&c->d_out, ((pl->la + pl->lb + 3) & ~(size_t)3) * 4)) != cudaSuccess)
+        return fail(bw_fail(BW_ENOMEM, "context allocation (%zu bytes of residues x2): %s",
+                            res_bytes, cudaGetErrorString(e)));
+    c->ntiles = (n / cpw + kCarryTileWords - 1) / kCarryTileWords;
+    c->state_bytes = 32 + c->ntiles * 16 + c->ntiles * 4;
+    if ((e = cudaMalloc(&c->d_state, c->state_bytes)) != cudaSuccess)
+        return fail(bw_fail(BW_ENOMEM, "carry state: %s", cudaGetErrorString(e)));
+    if ((e = cudaMemset(c->d_state, 0, c->state_bytes)) != cudaSuccess)
+        return fail(bw_fail(BW_ECUDA, "memset: %s", cudaGetErrorString(e)));
+    c->cst = reinterpret_cast<CarryState*>(c->d_state);
+    c->err = reinterpret_cast<uint32_t*>(c->d_state + 16);
+    c->rec_x = reinterpret_cast<uint4*>(c->d_state + 32);
+    c->rec_s = reinterpret_cast<uint32_t*>(c->d_state + 32 + c->ntiles * 16);
+    if ((e = cudaMallocHost(&c->h_err, 16)) != cudaSuccess)
+        return fail(bw_fail(BW_ENOMEM, "pinned: %s", cudaGetErrorString(e)));
+    for (auto& ev : c->ev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess)
+            return fail(bw_fail(BW_ECUDA, "event: %s", cudaGetErrorString(e)));
+    *out = c;
+    return BW_OK;
+}
+
+extern "C" int bw_ctx_destroy(bw_ctx* c) {
+    if (!c) return BW_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& ev : c->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    cudaFree(c->d_state);
+    cudaFree(c->d_out);
+    cudaFree(c->d_in);
+    cudaFree(c->d_res_b);
+    cudaFree(c->d_res_a);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return BW_OK;
+}
+
+extern "C" void* bw_ctx_stream(const bw_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+static int read_device_errors(bw_ctx* c) {
+    BW_CUDA(cudaMemcpyAsync(c->h_err, c->err, 4, cudaMemcpyDeviceToHost, c->stream));
+    BW_CUDA(cudaStreamSynchronize(c->stream));
+    const uint32_t e = *c->h_err;
+    if (e) {
+        BW_CUDA(cudaMemsetAsync(c->err, 0, 4, c->stream));
+        BW_CUDA(cudaStreamSynchronize(c->stream));
+        if (e & 1u)
+            return bw_fail(BW_ETIMEOUT, "carry look-back wait exceeded its bound (err=0x%x)", e);
+        return bw_fail(BW_ECHECK, "redundant-prime reconstruction check failed (err=0x%x)", e);
+    }
+    return BW_OK;
+}
+
+extern "C" int bw_ctx_set_wait_limit(bw_ctx* c, int polls) {
+    bw_clear_error();
+    if (!c || polls < 0) return bw_fail(BW_EINVAL, "bad argument");
+    c->spin_limit = polls;
+    return BW_OK;
+}
+
+extern "C" int bw_ctx_inject_wait_fault(bw_ctx* c, int enable) {
+    bw_clear_error();
+    if (!c) return bw_fail(BW_EINVAL, "NULL ctx");
+    c->inject_wait_fault = enable != 0;
+    return BW_OK;
+}
+
+extern "C" int bw_ctx_sync(bw_ctx* c) {
+    bw_clear_error();
+    if (!c) return bw_fail(BW_EINVAL, "NULL ctx");
+    BW_CUDA(cudaStreamSynchronize(c->stream));
+    return read_device_errors(c);
+}
+
+// ------------------------------------------------------------------ launch
+
+namespace {
+
+template <class Ar>
+const PlanDev<Ar>& plan_dev(const bw_plan* pl);
+template <>
+const PlanDev<Ar32>& plan_dev<Ar32>(const bw_plan* pl) {
+    return pl->pd32;
+}
+template <>
+const PlanDev<Ar64>& plan_dev<Ar64>(const bw_plan* pl) {
+    return pl->pd64;
+}
+
+constexpr int kMaxDynSmem = 200 * 1024;
+
+template <class Ar, bool SPLIT16>
+int set_smem_attrs() {
+    static std::once_flag once;
+    static cudaError_t st = cudaSuccess;
+    std::call_once(once, [] {
+        cudaError_t e1 = cudaFuncSetAttribute(k_fwd_col<Ar, SPLIT16>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              kMaxDynSmem);
+        cudaError_t e2 = cudaFuncSetAttribute(
+            k_row<Ar, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+        cudaError_t e3 = cudaFuncSetAttribute(
+            k_row<Ar, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+        cudaError_t e4 = cudaFuncSetAttribute(
+            k_inv_col<Ar>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+        st = e1 ? e1 : e2 ? e2 : e3 ? e3 : e4;
+    });
+    if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
+    return BW_OK;
+}
+
+// Enqueue K1..K3 (the transform part) for one product.
+template <class Ar, bool SPLIT16>
+int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool square,
+                      bool timing) {
+    using T = typename Ar::T;
+    const bw_plan* pl = c->plan;
+    const PlanDev<Ar>& pd = plan_dev<Ar>(pl);
+    int rc = set_smem_attrs<Ar, SPLIT16>();
+    if (rc) return rc;
+    const int R = 1 << pl->log_r, C = 1 << pl->log_c, CB = 1 << pl->log_cb;
+    T* ra = reinterpret_cast<T*>(c->d_res_a);
+    T* rb = reinterpret_cast<T*>(c->d_res_b);
+
+    const size_t smem1 = (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
+    dim3 g1(C / CB, 1, square ? 1 : 2);
+    const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
+    k_fwd_col<Ar, SPLIT16><<<g1, kColThreads, smem1, c->stream>>>(pd, a, pl->nca, b, pl->ncb,
+                                                                  ra, rb, zt);
+    if (timing) cudaEventRecord(c->ev[2], c->stream);
+
+    const size_t smem2 = (size_t)C * sizeof(T) * (square ? 1 : 2);
+    dim3 g2(R, pl->K);
+    if (pl->log_c >= 12) {
+        k_row<Ar, 512><<<g2, 512, smem2, c->stream>>>(pd, ra, square ? ra : rb, square ? 1 : 0);
+    } else {
+        k_row<Ar, 256><<<g2, 256, smem2, c->stream>>>(pd, ra, square ? ra : rb, square ? 1 : 0);
+    }
+    if (timing) cudaEventRecord(c->ev[3], c->stream);
+
+    const size_t smem3 = (size_t)R * CB * sizeof(T);
+    dim3 g3(C / CB, pl->K);
+    k_inv_col<Ar><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+    if (timing) cudaEventRecord(c->ev[4], c->stream);
+    BW_CUDA(cudaGetLastError());
+    return BW_OK;
+}
+
+template <class Ar, bool SPLIT16>
+int enqueue_carry(bw_ctx* c, uint32_t* out) {
+    using T = typename Ar::T;
+    const bw_plan* pl = c->plan;
+    const PlanDev<Ar>& pd = plan_dev<Ar>(pl);
+    const size_t n = (size_t)1 << pl->log_n;
+    const size_t NL = n / (SPLIT16 ? 2 : 1);
+    const size_t M = pl->la + pl->lb;
+    if (++c->epoch >= (1u << 28)) {
+        c->epoch = 1;
+        BW_CUDA(cudaMemsetAsync(c->d_state, 0, c->state_bytes, c->stream));
+    }
+    k_garner_carry<Ar, SPLIT16><<<(unsigned)c->ntiles, kCarryThreads, 0, c->stream>>>(
+        pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->cst, c->rec_x, c->rec_s,
+        c->epoch, c->inject_wait_fault ? c->epoch + (1u << 27) : c->epoch, c->err,
+        c->spin_limit);
+    BW_CUDA(cudaGetLastError());
+    return BW_OK;
+}
+
+int enqueue_product(bw_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                    bool square, bool timing) {
+    const bw_plan* pl = c->plan;
+    int rc;
+    if (pl->path == BW_PATH_P64) {
+        rc = enqueue_transform<Ar64, false>(c, a, b, square, timing);
+        if (!rc) rc = enqueue_carry<Ar64, false>(c, out);
+    } else {
+        rc = enqueue_transform<Ar32, true>(c, a, b, square, timing);
+        if (!rc) rc = enqueue_carry<Ar32, true>(c, out);
+    }
+    return rc;
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+}  // namespace
+
+static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
+                       uint32_t* out, size_t lc, unsigned flags, bw_timing* tm, bool square) {
+    bw_clear_error();
+    if (!c || !a || !out) return bw_fail(BW_EINVAL, "NULL argument");
+    const bw_plan* pl = c->plan;
+    if (square) {
+        b = a;
+        lb = la;
+    }
+    if (!b) return bw_fail(BW_EINVAL, "NULL b");
+    if (la != pl->la || lb != pl->lb)
+        return bw_fail(BW_EINVAL, "operand sizes %zu x %zu do not match the plan (%zu x %zu)", la,
+                       lb, pl->la, pl->lb);
+    const size_t M = la + lb;
+    if (lc < M) return bw_fail(BW_EINVAL, "output has %zu words, needs %zu", lc, M);
+    const bool sq = square || (a == b && la == lb);
+    const bool timing = tm != nullptr;
+    if (timing) cudaEventRecord(c->ev[0], c->stream);
+    int rc;
+    if (flags & BW_PTR_DEVICE) {
+        if (timing) cudaEventRecord(c->ev[1], c->stream);
+        rc = enqueue_product(c, a, b, out, sq, timing);
+        if (rc) return rc;
+        if (timing) {
+            cudaEventRecord(c->ev[5], c->stream);
+            cudaEventRecord(c->ev[6], c->stream);
+            BW_CUDA(cudaEventSynchronize(c->ev[6]));
+        }
+    } else {
+        BW_CUDA(cudaMemcpyAsync(c->d_in, a, la * 4, cudaMemcpyHostToDevice, c->stream));
+        const uint32_t* db = c->d_in;
+        if (!sq) {
+            BW_CUDA(cudaMemcpyAsync(c->d_in + la, b, lb * 4, cudaMemcpyHostToDevice, c->stream));
+            db = c->d_in + la;
+        }
+        if (timing) cudaEventRecord(c->ev[1], c->stream);
+        rc = enqueue_product(c, c->d_in, db, c->d_out, sq, timing);
+        if (rc) return rc;
+        if (timing) cudaEventRecord(c->ev[5], c->stream);
+        BW_CUDA(cudaMemcpyAsync(out, c->d_out, M * 4, cudaMemcpyDeviceToHost, c->stream));
+        if (timing) cudaEventRecord(c->ev[6], c->stream);
+        rc = read_device_errors(c);
+        if (rc) return rc;
+    }
+    if (timing) {
+        tm->h2d_ms = ev_ms(c->ev[0], c->ev[1]);
+        tm->fwd_ms = ev_ms(c->ev[1], c->ev[2]);
+        tm->mul_ms = ev_ms(c->ev[2], c->ev[3]);
+        tm->intt_ms = ev_ms(c->ev[3], c->ev[4]);
+        tm->crt_carry_ms = ev_ms(c->ev[4], c->ev[5]);
+        tm->d2h_ms = ev_ms(c->ev[5], c->ev[6]);
+        tm->total_ms = ev_ms(c->ev[0], c->ev[6]);
+    }
+    return BW_OK;
+}
+
+extern "C" int bw_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
+                           uint32_t* out, size_t lc, unsigned flags, bw_timing* tm) {
+    return do_multiply(c, a, la, b, lb, out, lc, flags, tm, false);
+}
+
+extern "C" int bw_square(bw_ctx* c, const uint32_t* a, size_t la, uint32_t* out, size_t lc,
+                         unsigned flags, bw_timing* tm) {
+    return do_multiply(c, a, la, nullptr, la, out, lc, flags, tm, true);
+}
+
+// ------------------------------------------------------------------ Garner dump
+
+namespace {
+template <class Ar, bool SPLIT16>
+__global__ void k_garner_dump(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
+                              uint32_t* __restrict__ words, size_t n) {
+    using T = typename Ar::T;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Ar a1 = P.pr[1].ar;
+    const GarnerDev<Ar>& G = P.gar;
+    const T r0 = res[i], r1 = res[n + i];
+    const T r0m1 = a1.red1(a1.shoup(r0, 1, P.pr[1].one_q));
+    const T t1 = r1 >= r0m1 ? r1 - r0m1 : r1 + a1.p - r0m1;
+    const T k1 = a1.red1(a1.shoup(t1, G.inv1, G.inv1q));
+    const unsigned __int128 x = (unsigned __int128)G.p0 * k1 + r0;
+    words[3 * i] = (uint32_t)x;
+    words[3 * i + 1] = (uint32_t)(x >> 32);
+    words[3 * i + 2] = (uint32_t)(x >> 64);
+}
+}  // namespace
+
+extern "C" int bw_multiply_coeffs(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* b,
+                                  size_t lb, uint32_t* words, size_t n_words) {
+    bw_clear_error();
+    if (!c || !a || !b || !words) return bw_fail(BW_EINVAL, "NULL argument");
+    const bw_plan* pl = c->plan;
+    if (la != pl->la || lb != pl->lb) return bw_fail(BW_EINVAL, "operand sizes do not match plan");
+    const size_t n = (size_t)1 << pl->log_n;
+    if (n_words < 3 * n) return bw_fail(BW_EINVAL, "words needs 3*n = %zu entries", 3 * n);
+    uint32_t* d_words = nullptr;
+    BW_CUDA(cudaMalloc(&d_words, 3 * n * 4));
+    int rc = BW_OK;
+    const bool sq = (a == b && la == lb);
+    cudaMemcpyAsync(c->d_in, a, la * 4, cudaMemcpyHostToDevice, c->stream);
+    if (!sq) cudaMemcpyAsync(c->d_in + la, b, lb * 4, cudaMemcpyHostToDevice, c->stream);
+    const uint32_t* db = sq ? c->d_in : c->d_in + la;
+    if (pl->path == BW_PATH_P64) {
+        rc = enqueue_transform<Ar64, false>(c, c->d_in, db, sq, false);
+        if (!rc)
+            k_garner_dump<Ar64, false><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+                pl->pd64, reinterpret_cast<const uint64_t*>(c->d_res_a), d_words, n);
+    } else {
+        rc = enqueue_transform<Ar32, true>(c, c->d_in, db, sq, false);
+        if (!rc)
+            k_garner_dump<Ar32, true><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+                pl->pd32, reinterpret_cast<const uint32_t*>(c->d_res_a), d_words, n);
+    }
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(words, d_words, 3 * n * 4, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = bw_fail(BW_ECUDA, "coeff dump: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_words);
+    return rc;
+}
+
+// ------------------------------------------------------------------ misc ABI
+
+extern "C" int bw_abi_version(void) { return BW_ABI_VERSION; }
+
+extern "C" const char* bw_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int bw_limits(int path, int num_primes, bw_limits_info* o) {
+    bw_clear_error();
+    if (!o) return bw_fail(BW_EINVAL, "NULL out");
+    if (path == BW_PATH_AUTO) path = BW_PATH_P64;
+    if (path != BW_PATH_P32 && path != BW_PATH_P64) return bw_fail(BW_EINVAL, "unknown path");
+    const int K = num_primes == 0 ? 2 : num_primes;
+    if (K < 2 || K > 3) return bw_fail(BW_EINVAL, "num_primes must be 2 or 3");
+    o->path = path;
+    o->num_primes = K;
+    o->max_log_n = bw_path_max_log_n(path, K);
+    const int cpw = path == BW_PATH_P32 ? 2 : 1;
+    o->max_square_words = ((size_t)1 << (o->max_log_n - 1)) / cpw;
+    return BW_OK;
+}
+
+extern "C" int bw_size_supported(int path, int num_primes, size_t la, size_t lb) {
+    bw_clear_error();
+    if (path == BW_PATH_AUTO) path = choose_path(la, lb);
+    return bw_check_size(path, num_primes == 0 ? 2 : num_primes, la, lb, nullptr);
+}
+
+extern "C" int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
+                                     uint32_t* c, size_t lc, int path, float* elapsed_ms) {
+    const auto t0 = std::chrono::high_resolution_clock::now();
+    bw_plan* pl = nullptr;
+    int rc = bw_plan_create(&pl, path, la, lb, 0, 0);
+    if (rc) return rc;
+    bw_ctx* cx = nullptr;
+    rc = bw_ctx_create(&cx, pl, nullptr);
+    if (!rc) rc = bw_multiply(cx, a, la, b, lb, c, lc, BW_PTR_HOST, nullptr);
+    std::string err = rc ? g_last_error : std::string();
+    bw_ctx_destroy(cx);
+    bw_plan_destroy(pl);
+    if (rc) g_last_error = err;
+    const auto t1 = std::chrono::high_resolution_clock::now();
+    if (elapsed_ms) *elapsed_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    return rc;
+}

@@ -1,0 +1,198 @@
+/*
+ * birdwing.h -- C ABI of the B200-native big-integer multiply library
+ * (libbirdwing.so).
+ *
+ * Multiplies large unsigned integers given as little-endian arrays of 32-bit
+ * words ("limbs") with a residue-number-system NTT pipeline on one NVIDIA
+ * B200 (sm_100a):
+ *
+ *   limb split + zero pad -> forward NTT per prime -> pointwise product ->
+ *   inverse NTT -> Garner CRT reconstruction -> carry propagation.
+ *
+ * Two prime paths are compiled into the same library and chosen at run time:
+ *
+ *   BW_PATH_P32 : 16-bit coefficients, 30-bit primes, 32-bit modular
+ *                 arithmetic (the reference's LIMB_BITS=32 pipeline, whose
+ *                 transform length is twice the limb count).
+ *   BW_PATH_P64 : 32-bit coefficients, 62-bit primes of the form c*2^32+1,
+ *                 64-bit modular arithmetic (the reference's LIMB_BITS=64
+ *                 "hybrid" and NATIVE_HOST_LIMBS pipelines; a u64 limb array
+ *                 is passed as twice as many u32 words).
+ *
+ * Everything crossing this boundary is a plain pointer, size or POD struct.
+ * Every call returns an int status (BW_OK == 0, negative on error); the
+ * library never calls exit().  bw_last_error() returns a thread-local
+ * message for the most recent failure on the calling thread.
+ *
+ * Reference interfaces this ABI replaces (paths inside nikitaborisov/birdwing):
+ *   host_multiply_merge / host_multiply_merge_native  include/multiply.h:9-23,
+ *       src/host_multiply.cpp:27-134              -> bw_multiply_host_once
+ *   precompute_ntt + upload_ntt_precomputed           include/gpu_ntt.h:101-102,
+ *       src/gpu_ntt.cu:240-379                      -> bw_plan_create
+ *   allocate_ntt_context                              include/gpu_ntt.h:103,
+ *       src/gpu_ntt.cu:382-440                      -> bw_ctx_create
+ *   execute_ntt_multiply                              include/gpu_ntt.h:105-115,
+ *       src/gpu_ntt.cu:442-973                      -> bw_multiply / bw_square
+ *   execute_ntt_multiply(..., crt_*_out)              src/gpu_ntt.cu:843-884
+ *                                                   -> bw_multiply_coeffs
+ *   cleanup_ntt_context / cleanup_ntt_precomputed     include/gpu_ntt.h:117-118
+ *                                                   -> bw_ctx_destroy / bw_plan_destroy
+ *   ntt_limits family                                 include/ntt_limits.h:9-31,
+ *       src/ntt_limits.cpp:14-280                   -> bw_limits
+ *   NTTTiming                                         include/gpu_ntt.h:87-99
+ *                                                   -> bw_timing
+ */
+#ifndef BIRDWING_H
+#define BIRDWING_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BW_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define BW_OK            0
+#define BW_EINVAL      (-1)  /* bad argument (null pointer, zero length, ...) */
+#define BW_ENOMEM      (-2)  /* device or pinned-host allocation failed       */
+#define BW_ECUDA       (-3)  /* a CUDA runtime call failed                    */
+#define BW_ETIMEOUT    (-4)  /* a bounded device-side wait gave up            */
+#define BW_EREJECT     (-5)  /* admission rejected (memory budget)            */
+#define BW_ESIZE       (-6)  /* product size outside the supported limits     */
+#define BW_ECHECK      (-7)  /* redundant-prime consistency check failed      */
+#define BW_EBUSY       (-8)  /* resource still in use                         */
+
+/* ---- prime paths --------------------------------------------------------- */
+#define BW_PATH_AUTO   0
+#define BW_PATH_P32    32
+#define BW_PATH_P64    64
+
+/* ---- flags for bw_multiply ------------------------------------------------ */
+#define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
+                                the call copies in, computes, copies out and
+                                synchronises                                 */
+#define BW_PTR_DEVICE  1u    /* a, b, c are device pointers: the call only
+                                enqueues work on the context's stream        */
+
+/* Opaque handles.  A plan owns the per-size device tables (twiddles, Garner
+ * constants); a context owns device scratch and a stream and borrows its
+ * plan's tables (the reference's NTTContext borrows NTTPrecomputed's device
+ * pointers the same way, src/gpu_ntt.cu:398-402).  Distinct handles may be
+ * used from distinct threads; one context is used by one thread at a time. */
+typedef struct bw_plan bw_plan;
+typedef struct bw_ctx bw_ctx;
+
+/* Per-stage device times in milliseconds (CUDA events on the context stream).
+ * Field meanings follow the reference's NTTTiming (include/gpu_ntt.h:87-99):
+ * fwd_ms covers limb split + zero pad + forward column pass for both operands;
+ * mul_ms the fused row pass (forward rows, pointwise product, inverse rows);
+ * intt_ms the inverse column pass; crt_carry_ms the fused Garner + carry. */
+typedef struct bw_timing {
+    float h2d_ms;
+    float fwd_ms;
+    float mul_ms;
+    float intt_ms;
+    float crt_carry_ms;
+    float d2h_ms;
+    float total_ms;
+} bw_timing;
+
+typedef struct bw_plan_info {
+    int      path;          /* BW_PATH_P32 or BW_PATH_P64                    */
+    int      num_primes;    /* K                                             */
+    int      log_n;         /* transform length n = 2^log_n                  */
+    int      log_rows;      /* 4-step split n = rows * cols                   */
+    int      log_cols;
+    int      coeff_bits;    /* 16 or 32                                      */
+    size_t   la, lb;        /* operand lengths in u32 words                  */
+    size_t   lc;            /* product length in u32 words (= la + lb)       */
+    size_t   plan_device_bytes;   /* twiddle + constant tables               */
+    size_t   ctx_device_bytes;    /* scratch one context allocates           */
+    uint64_t primes[3];
+} bw_plan_info;
+
+typedef struct bw_limits_info {
+    int      path;
+    int      num_primes;
+    int      max_log_n;        /* largest transform length supported         */
+    size_t   max_square_words; /* largest la == lb (u32 words)               */
+} bw_limits_info;
+
+/* Returns BW_ABI_VERSION. */
+int bw_abi_version(void);
+
+/* Message describing the last failure on this thread ("" if none). */
+const char* bw_last_error(void);
+
+/* Limits of one prime path.  num_primes = 0 selects the default K. */
+int bw_limits(int path, int num_primes, bw_limits_info* out);
+
+/* Would a product of la x lb u32 words be accepted?  Returns BW_OK or
+ * BW_ESIZE with a reason in bw_last_error().  (Reference:
+ * multiply_size_supported, src/ntt_limits.cpp:232-245.) */
+int bw_size_supported(int path, int num_primes, size_t la, size_t lb);
+
+/* Build the plan (twiddle tables on the device, Garner constants) for
+ * products of la x lb u32 words.  path = BW_PATH_AUTO picks the faster path
+ * for the size; num_primes = 0 picks the smallest K whose product bound
+ * holds (2 for both paths).  The plan is bound to the current CUDA device. */
+int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb,
+                   int num_primes, unsigned flags);
+int bw_plan_destroy(bw_plan* plan);
+int bw_plan_get_info(const bw_plan* plan, bw_plan_info* out);
+
+/* Allocate device scratch for one in-flight product of the plan's size.
+ * stream = NULL creates a private non-blocking stream; otherwise work is
+ * issued on the given cudaStream_t. */
+int bw_ctx_create(bw_ctx** out, const bw_plan* plan, void* stream);
+int bw_ctx_destroy(bw_ctx* ctx);
+/* The cudaStream_t the context issues work on. */
+void* bw_ctx_stream(const bw_ctx* ctx);
+/* Wait for the context's stream and report device-side errors raised by
+ * earlier BW_PTR_DEVICE calls (BW_ETIMEOUT, BW_ECHECK). */
+int bw_ctx_sync(bw_ctx* ctx);
+
+/* c[0 .. la+lb) = a[0 .. la) * b[0 .. lb).  lc must be >= la + lb; words of
+ * c beyond la + lb are left untouched.  la and lb must equal the plan's.
+ * a == b with la == lb multiplies a number by itself through the squaring
+ * schedule (one forward transform).  timing may be NULL. */
+int bw_multiply(bw_ctx* ctx, const uint32_t* a, size_t la,
+                const uint32_t* b, size_t lb, uint32_t* c, size_t lc,
+                unsigned flags, bw_timing* timing);
+
+/* c = a * a with the squaring schedule. */
+int bw_square(bw_ctx* ctx, const uint32_t* a, size_t la,
+              uint32_t* c, size_t lc, unsigned flags, bw_timing* timing);
+
+/* Stop after Garner: the n convolution coefficients of the product (in the
+ * plan's coefficient base, 2^16 or 2^32) as three little-endian u32 words
+ * each, words[3*i + w].  Host pointers only.  (Reference: the CRT dump of
+ * execute_ntt_multiply, src/gpu_ntt.cu:843-884.) */
+int bw_multiply_coeffs(bw_ctx* ctx, const uint32_t* a, size_t la,
+                       const uint32_t* b, size_t lb, uint32_t* words,
+                       size_t n_words);
+
+/* Test hooks for the bounded device-side waits of the carry look-back.
+ * bw_ctx_set_wait_limit sets how many polls (about 64 ns apart) a wait may
+ * take before it gives up and the call reports BW_ETIMEOUT (default 2^22).
+ * bw_ctx_inject_wait_fault(ctx, 1) makes the next products wait for a tile
+ * flag that nothing sets, so every wait runs out; the context stays usable
+ * and products are correct again after bw_ctx_inject_wait_fault(ctx, 0).
+ * No counterpart in the reference (it checks no CUDA errors at all). */
+int bw_ctx_set_wait_limit(bw_ctx* ctx, int polls);
+int bw_ctx_inject_wait_fault(bw_ctx* ctx, int enable);
+
+/* One-shot convenience: plan + context + multiply + teardown, host pointers.
+ * (Reference: host_multiply_merge, src/host_multiply.cpp:27-86.) */
+int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b,
+                          size_t lb, uint32_t* c, size_t lc, int path,
+                          float* elapsed_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BIRDWING_H */

@@ -1,0 +1,74 @@
+"""The C-ABI library loads, exports every function include/birdwing.h
+declares, and its host-side admission logic behaves like the reference's
+ntt_limits (no GPU calls here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import birdwing_b200 as bw
+from birdwing_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "birdwing.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(bw_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 15
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, n
+
+
+def test_abi_version():
+    assert bw.lib.bw_abi_version() == 1
+
+
+def test_limits():
+    l64 = bw.limits(bw.BW_PATH_P64)
+    l32 = bw.limits(bw.BW_PATH_P32)
+    assert l64["max_log_n"] >= 24 and l64["num_primes"] == 2
+    assert l32["max_log_n"] == 24
+    assert l32["max_square_words"] == (1 << 23) // 2
+    assert bw.limits(bw.BW_PATH_P64, 3)["num_primes"] == 3
+
+
+@pytest.mark.parametrize("la,lb,path,ok", [
+    (1, 1, 64, True), (1 << 23, 1 << 23, 64, True), (1 << 15, 1 << 15, 32, True),
+    (1 << 23, 1 << 23, 32, False),   # 2^24 16-bit coefficients each -> n = 2^25
+    (0, 5, 64, False), (5, 0, 32, False),
+])
+def test_size_supported(la, lb, path, ok):
+    good, why = bw.size_supported(la, lb, path)
+    assert good == ok
+    if not ok:
+        assert why
+
+
+def test_bad_arguments_are_reported_not_fatal():
+    h = ctypes.c_void_p()
+    assert bw.lib.bw_plan_create(ctypes.byref(h), 17, 4, 4, 0, 0) == _lib.BW_EINVAL
+    assert "path" in _lib.last_error()
+    assert bw.lib.bw_plan_create(ctypes.byref(h), 64, 4, 4, 5, 0) == _lib.BW_EINVAL
+    assert bw.lib.bw_plan_create(ctypes.byref(h), 64, 0, 4, 0, 0) == _lib.BW_ESIZE
+    assert bw.lib.bw_plan_create(None, 64, 4, 4, 0, 0) == _lib.BW_EINVAL
+    with pytest.raises(bw.BwError) as e:
+        bw.Plan(1 << 26, 1 << 26, bw.BW_PATH_P64)
+    assert e.value.code == _lib.BW_ESIZE
+
+
+def test_limb_conversions():
+    import numpy as np
+    x = (1 << 200) + 12345
+    w = bw.int_to_limbs(x)
+    assert w.dtype == np.uint32 and bw.limbs_to_int(w) == x
+    assert bw.limbs_to_int(bw.int_to_limbs(7, 4)) == 7
+    assert bw.limbs_to_int(np.array([1, 2], dtype=np.uint64)) == 1 + (2 << 64)

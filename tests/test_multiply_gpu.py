@@ -1,0 +1,263 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and GMP.
+
+Bit-exact everywhere: this is integer arithmetic.  Small and medium sizes
+are checked against the oracle (the CPU restatement of the reference's
+algorithm) and GMP; the BASELINE sizes against GMP and through
+size-independent properties (squaring == self-product, linearity in one
+operand, products mod small primes)."""
+import os
+
+import numpy as np
+import pytest
+
+import birdwing_b200 as bw
+from oracle import gmp_ref, mt64, oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "fixtures.npz"))
+PATHS = [(64, 2), (64, 3), (32, 2), (32, 3)]
+
+
+def as_int(w):
+    return int.from_bytes(np.ascontiguousarray(w).view(np.uint8).tobytes(), "little")
+
+
+def gpu_mul(a, b, path=64, K=2):
+    with bw.Plan(len(a), len(b), path, K) as p, bw.Context(p) as c:
+        return c.multiply(a, b)
+
+
+def rand_words(n, rng, top=True):
+    w = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    if top:
+        w[-1] |= np.uint32(0x80000000)
+    return w
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_golden_reference_pattern_u32(path, K):
+    # tests/test_full_multiply.cpp:245-265 (test_full_pipeline sizes)
+    for L in (4, 8, 16, 64, 128, 2048, 10000):
+        a, b, c = GOLD[f"ref32_{L}_a"], GOLD[f"ref32_{L}_b"], GOLD[f"ref32_{L}_c"]
+        assert (gpu_mul(a, b, path, K) == c).all(), L
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_golden_reference_pattern_u64(path, K):
+    # tests/test_full_multiply.cpp:482-518 (64-bit limbs incl. UINT64_MAX)
+    for L in (4, 16, 64, 256, 1024, 4096):
+        a, b, c = GOLD[f"ref64_{L}_a"], GOLD[f"ref64_{L}_b"], GOLD[f"ref64_{L}_c"]
+        got = gpu_mul(a.view(np.uint32), b.view(np.uint32), path, K)
+        assert (got.view(np.uint64) == c).all(), L
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_golden_unbalanced(path, K):
+    for stem in ("top_1000x125", "top_4096x4096", "top_777x3001"):
+        a, b, c = GOLD[stem + "_a"], GOLD[stem + "_b"], GOLD[stem + "_c"]
+        assert (gpu_mul(a, b, path, K) == c).all(), stem
+
+
+def test_reference_simple_cases():
+    # tests/test_full_multiply.cpp:268-287
+    one = np.array([1, 0, 0, 0], dtype=np.uint32)
+    z = np.zeros(4, dtype=np.uint32)
+    f = np.array([42, 0, 0, 0], dtype=np.uint32)
+    for path, K in PATHS:
+        assert as_int(gpu_mul(one, one, path, K)) == 1
+        assert as_int(gpu_mul(z, f, path, K)) == 0
+        # root-of-unity probe, L = 8 (:307-351): A[1] = 1, B[0] = 1
+        a = np.zeros(8, dtype=np.uint32)
+        b = np.zeros(8, dtype=np.uint32)
+        a[1] = 1
+        b[0] = 1
+        c = gpu_mul(a, b, path, K)
+        assert c[1] == 1 and as_int(c) == 1 << 32
+
+
+def test_identities_large():
+    # tests/test_full_multiply.cpp:289-305 at L = 2^20
+    L = 1 << 20
+    Z = np.zeros(L, dtype=np.uint32)
+    O = np.ones(L, dtype=np.uint32)
+    for path, K in ((64, 2), (32, 3)):
+        assert not gpu_mul(Z, Z, path, K).any()
+        assert not gpu_mul(O, Z, path, K).any()
+        r = gpu_mul(O, O, path, K)
+        assert r[0] == 1
+        assert (r == gmp_ref.mul(O, O)).all()
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_sizes_sweep_vs_oracle(path, K):
+    rng = np.random.default_rng(100 + path + K)
+    shapes = [(1, 1), (1, 2), (2, 1), (3, 5), (7, 7), (8, 8), (9, 8), (15, 17), (16, 16),
+              (31, 33), (100, 3), (3, 100), (255, 256), (256, 256), (257, 255), (1000, 1),
+              (1023, 1025), (2048, 2048), (4095, 4097), (5000, 300)]
+    for la, lb in shapes:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = oracle.multiply(a, b, path, K)
+        assert (gpu_mul(a, b, path, K) == want).all(), (la, lb)
+
+
+def test_sizes_sweep_vs_gmp_medium():
+    rng = np.random.default_rng(7)
+    for la, lb in [(1 << 14, 1 << 14), ((1 << 16) + 3, (1 << 15) - 5), (1 << 17, 1 << 10),
+                   (123457, 98765), (1 << 19, 1 << 19)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = gmp_ref.mul(a, b)
+        for path, K in ((64, 2), (64, 3), (32, 2)):
+            assert (gpu_mul(a, b, path, K) == want).all(), (la, lb, path, K)
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_carry_stress_all_ones(path, K):
+    # (2^(32m) - 1)^2 and (2^(32m)-1)(2^(32m)+1): long runs of 0xFFFFFFFF words
+    # force propagate chains through many carry tiles
+    for m in (1, 7, 2048, 2049, 1 << 15):
+        a = np.full(m, 0xFFFFFFFF, dtype=np.uint32)
+        assert (gpu_mul(a, a, path, K) == gmp_ref.mul(a, a)).all(), m
+        b = np.zeros(m + 1, dtype=np.uint32)
+        b[0] = 1
+        b[m] = 1
+        if (m + m + 1) * (2 if path == 32 else 1) <= (1 << 24):
+            got = gpu_mul(a, b, path, K)
+            assert (got == gmp_ref.mul(a, b)).all(), m
+
+
+@pytest.mark.parametrize("path,K", [(64, 2), (32, 3)])
+def test_square_paths(path, K):
+    rng = np.random.default_rng(11)
+    for L in (1, 5, 64, 1000, 4096, 1 << 16):
+        a = rand_words(L, rng)
+        want = gmp_ref.mul(a, a)
+        with bw.Plan(L, L, path, K) as p, bw.Context(p) as c:
+            assert (c.square(a) == want).all(), L
+            assert (c.multiply(a, a) == want).all(), L   # same array: squaring schedule
+            b = a.copy()
+            assert (c.multiply(a, b) == want).all(), L   # distinct arrays: full schedule
+
+
+def test_context_reuse_and_timing():
+    rng = np.random.default_rng(3)
+    L = 1 << 12
+    with bw.Plan(L, L, 64) as p, bw.Context(p) as c:
+        for _ in range(5):
+            a, b = rand_words(L, rng), rand_words(L, rng)
+            out, t = c.multiply(a, b, timing=True)
+            assert (out == gmp_ref.mul(a, b)).all()
+            assert t["total_ms"] > 0 and t["fwd_ms"] >= 0
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_crt_coefficient_dump(path, K):
+    # the reference's CRT dump (src/gpu_ntt.cu:843-884): convolution
+    # coefficients before carry, compared with the oracle's per-prime
+    # convolutions joined by the oracle's Garner
+    rng = np.random.default_rng(5)
+    for la, lb in ((3, 5), (100, 77), (1000, 1000)):
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        with bw.Plan(la, lb, path, K) as p, bw.Context(p) as c:
+            got = c.coeffs(a, b)
+            n = p.N
+        per = 2 if path == 32 else 1
+        ca = [int(x) for x in (a.view(np.uint16) if per == 2 else a)]
+        cb = [int(x) for x in (b.view(np.uint16) if per == 2 else b)]
+        primes, roots, logs = oracle.path_basis(path)
+        log_n = n.bit_length() - 1
+        res = []
+        for k in range(K):
+            w = oracle.lib.oracle_root_for(primes[k], roots[k], logs[k], log_n)
+            res.append(oracle.conv_mod(ca, cb, primes[k], w, n))
+        want = [oracle.garner([int(r[i]) for r in res], primes[:K]) for i in range(n)]
+        assert got == want
+        # and the coefficients are the exact linear convolution
+        lin = [0] * n
+        for i, x in enumerate(ca):
+            if x:
+                for j, y in enumerate(cb):
+                    lin[i + j] += x * y
+        assert got == lin
+
+
+def test_device_pointers_torch():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(9)
+    la, lb = 50000, 30001
+    a, b = rand_words(la, rng), rand_words(lb, rng)
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.zeros(la + lb + 5, dtype=torch.int32, device="cuda")
+    with bw.Plan(la, lb, 64) as p, bw.Context(p) as c:
+        c.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, dc.data_ptr() + 4, la + lb)
+        c.sync()
+        got = dc.cpu().numpy().view(np.uint32)
+    assert got[0] == 0 and (got[1:1 + la + lb] == gmp_ref.mul(a, b)).all()
+    assert not got[1 + la + lb:].any()
+
+
+def test_wrong_sizes_are_rejected():
+    with bw.Plan(8, 8, 64) as p, bw.Context(p) as c:
+        with pytest.raises(bw.BwError) as e:
+            c.multiply(np.ones(9, dtype=np.uint32), np.ones(8, dtype=np.uint32))
+        assert e.value.code == -1
+        # the context still works afterwards
+        a = np.arange(1, 9, dtype=np.uint32)
+        assert (c.multiply(a, a) == gmp_ref.mul(a, a)).all()
+
+
+def test_lookback_wait_fault_is_reported_and_recoverable():
+    # inject a look-back flag that nothing sets: every bounded wait runs out,
+    # the call returns BW_ETIMEOUT instead of hanging, the context survives
+    import ctypes
+    rng = np.random.default_rng(4)
+    L = 1 << 16
+    a, b = rand_words(L, rng), rand_words(L, rng)
+    want = gmp_ref.mul(a, b)
+    with bw.Plan(L, L, 64) as p, bw.Context(p) as c:
+        assert (c.multiply(a, b) == want).all()
+        assert bw.lib.bw_ctx_set_wait_limit(c._h, 200) == 0
+        assert bw.lib.bw_ctx_inject_wait_fault(c._h, 1) == 0
+        with pytest.raises(bw.BwError) as e:
+            c.multiply(a, b)
+        assert e.value.code == -4
+        assert bw.lib.bw_ctx_inject_wait_fault(c._h, 0) == 0
+        assert bw.lib.bw_ctx_set_wait_limit(c._h, 1 << 22) == 0
+        assert (c.multiply(a, b) == want).all()
+        del ctypes
+
+
+def test_config1_plain_small():
+    # 2^20-bit operands (2^15 words), 16-bit
+    # coefficients, n = 2^17, three 30-bit primes
+    a = mt64.random_words_top(1 << 15, 1234)
+    b = mt64.random_words_top(1 << 15, 5678)
+    with bw.Plan(a.size, b.size, 32, 3) as p, bw.Context(p) as c:
+        assert p.info["log_n"] == 17 and p.info["num_primes"] == 3
+        assert (c.multiply(a, b) == gmp_ref.mul(a, b)).all()
+
+
+def test_config2_plain_large():
+    # 2^28-bit operands (2^23 words), 32-bit
+    # coefficients, n = 2^24, 62-bit primes; plus the squaring variant
+    a = mt64.random_words_top_fast(1 << 23, 1234)
+    b = mt64.random_words_top_fast(1 << 23, 5678)
+    with bw.Plan(a.size, b.size, 64, 2) as p, bw.Context(p) as c:
+        assert p.info["log_n"] == 24
+        got = c.multiply(a, b)
+        sq = c.square(a)
+    assert (got == gmp_ref.mul(a, b)).all()
+    assert (sq == gmp_ref.mul(a, a)).all()
+
+
+def test_config2_three_primes_properties():
+    # size-independent checks at the full size: residues of the product mod
+    # small primes and mod 2^64 equal the products of the operands' residues
+    a = mt64.random_words_top_fast(1 << 23, 42)
+    b = mt64.random_words_top_fast(1 << 23, 43)
+    got = gpu_mul(a, b, 64, 3)
+    A, B, C = as_int(a), as_int(b), as_int(got)
+    for m in (2 ** 64, 2 ** 61 - 1, 1000000007, 998244353, (1 << 31) - 1):
+        assert C % m == (A % m) * (B % m) % m
+    assert C.bit_length() <= 64 * (1 << 23)
