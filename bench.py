@@ -43,6 +43,9 @@ CONFIGS = {
             "squaring 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
     "1": (1 << 15, 1 << 15, 32, 3, False,
           "plain 2^20-bit x 2^20-bit, 16-bit coefficients, n=2^17, 3 x 30-bit primes"),
+    # a smaller product of the same kernels for ncu captures (working set > L2)
+    "prof": (1 << 21, 1 << 21, 64, 2, False,
+             "plain 2^26-bit x 2^26-bit, 32-bit coefficients, n=2^22, 2 x 62-bit primes"),
 }
 
 
@@ -55,6 +58,10 @@ def parse():
     ap.add_argument("--config", default="2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--log-cols", type=int, default=0,
+                    help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")
+    ap.add_argument("--plan-flags", type=lambda s: int(s, 0), default=0,
+                    help="extra bw_plan_create flags (tuning switches)")
     return ap.parse_args()
 
 
@@ -241,7 +248,7 @@ def main():
 
     la, lb, path, K, square, desc = CONFIGS[args.config]
     a, b = operands(args.config, rank)
-    plan = bw.Plan(la, lb, path, K)
+    plan = bw.Plan(la, lb, path, K, log_cols=args.log_cols, flags=args.plan_flags)
     ctx = bw.Context(plan)
     stream = torch.cuda.ExternalStream(ctx.stream)
     n = plan.N
@@ -332,6 +339,7 @@ def main():
             "vs_baseline": None, "dtype": "u64" if path == 64 else "u32", "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "words_a": la,
                        "words_b": lb, "path": path, "num_primes": K, "log_n": plan.logN,
+                       "log_cols": plan.info["log_cols"], "plan_flags": args.plan_flags,
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "correct_vs_gmp": ok,

@@ -27,6 +27,9 @@ BW_PATH_P64 = 64
 BW_PTR_HOST = 0
 BW_PTR_DEVICE = 1
 
+BW_PLAN_RADIX8 = 1 << 16
+BW_PLAN_TW_GLOBAL = 1 << 17
+
 _NAMES = {
     BW_EINVAL: "BW_EINVAL", BW_ENOMEM: "BW_ENOMEM", BW_ECUDA: "BW_ECUDA",
     BW_ETIMEOUT: "BW_ETIMEOUT", BW_EREJECT: "BW_EREJECT", BW_ESIZE: "BW_ESIZE",

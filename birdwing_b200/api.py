@@ -78,9 +78,10 @@ def size_supported(la, lb, path=L.BW_PATH_AUTO, num_primes=0):
 class Plan:
     """Per-size tables on the device (twiddles, Garner constants)."""
 
-    def __init__(self, la, lb, path=L.BW_PATH_AUTO, num_primes=0):
+    def __init__(self, la, lb, path=L.BW_PATH_AUTO, num_primes=0, log_cols=0, flags=0):
         h = ctypes.c_void_p()
-        check(lib.bw_plan_create(ctypes.byref(h), path, la, lb, num_primes, 0))
+        flags = flags | ((log_cols & 0x1F) << 8)
+        check(lib.bw_plan_create(ctypes.byref(h), path, la, lb, num_primes, flags))
         self._h = h
         info = L.bw_plan_info()
         check(lib.bw_plan_get_info(self._h, ctypes.byref(info)))

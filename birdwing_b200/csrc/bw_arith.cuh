@@ -32,8 +32,8 @@ struct Ar32 {
     uint32_t p2;    // 2p
     uint32_t pinv;  // -p^-1 mod 2^32
 
-    __device__ __forceinline__ T red2(T a) const { return a >= p2 ? a - p2 : a; }
-    __device__ __forceinline__ T red1(T a) const { return a >= p ? a - p : a; }
+    __device__ __forceinline__ T red2(T a) const { return min(a, a - p2); }
+    __device__ __forceinline__ T red1(T a) const { return min(a, a - p); }
     // x < 2^32, w < p: returns x*w mod p in [0, 2p)
     __device__ __forceinline__ T shoup(T x, T w, T wq) const {
         const uint32_t q = __umulhi(x, wq);
@@ -59,20 +59,84 @@ struct Ar32 {
         a = red2(u);
         b = shoup(v, w, wq);
     }
+    // twiddle-1 butterflies of stage 0 (inputs known to be in [0, 2p))
+    __device__ __forceinline__ void ct1(T& a, T& b) const {
+        const T x = a;
+        a = x + b;
+        b = x - b + p2;
+    }
+    __device__ __forceinline__ void gs1(T& a, T& b) const {
+        const T x = a;
+        a = red2(x + b);
+        b = red2(x - b + p2);
+    }
+    // forward-transform output range [0, 4p) -> [0, 2p)
+    __device__ __forceinline__ T fwd_to_2p(T a) const { return red2(a); }
+    // Shoup companion floor(w 2^32 / p) of w < p
+    __device__ __forceinline__ T companion(T w) const {
+        return (uint32_t)((((uint64_t)w) << 32) / p);
+    }
 };
 
+// The 64-bit path's primes are p = c 2^32 + 1 with 2^61 <= p < 2^64 / 6 (62
+// bits).  The forward (CT) transform keeps values in [0, 6p + 2^32): its
+// Shoup quotient omits the x0*v0 partial product (q may be 2 short, so the
+// product lies in [0, 3p)), and its input reduction compares the high word
+// only (subtract 3p when hi > 3c).  The inverse (GS) transform uses the exact
+// quotient and keeps values in [0, 2p).
 struct Ar64 {
     using T = uint64_t;
     static constexpr int BITS = 64;
     uint64_t p;
     uint64_t p2;    // 2p
     uint64_t pinv;  // -p^-1 mod 2^64
+    uint32_t c;     // p = c * 2^32 + 1
+    uint32_t c3;    // 3c
+    uint64_t p3;    // 3p
+    uint64_t p4;    // 4p
+    uint64_t mu_lo; // floor(2^128 / p) = mu_hi 2^64 + mu_lo
+    uint32_t mu_hi;
 
-    __device__ __forceinline__ T red2(T a) const { return a >= p2 ? a - p2 : a; }
-    __device__ __forceinline__ T red1(T a) const { return a >= p ? a - p : a; }
+    __device__ __forceinline__ T red2(T a) const { return min(a, a - p2); }
+    __device__ __forceinline__ T red1(T a) const { return min(a, a - p); }
+    // x < 2^64, w < p: x*w mod p in [0, 2p).  The quotient q = hi64(x * wq)
+    // is exact and built from 32x32->64 multiply-adds (mad.wide.u32) whose
+    // 64-bit addends never overflow:
+    //   T = x0 v1 + hi(x0 v0),  W = x1 v0 + lo(T),  q = x1 v1 + hi(W) + hi(T).
+    // Because p = c 2^32 + 1, q*p mod 2^64 = q + (q0 c) 2^32 costs one
+    // multiply-add; r = lo64(x w) - lo64(q p).
     __device__ __forceinline__ T shoup(T x, T w, T wq) const {
-        const uint64_t q = __umul64hi(x, wq);
-        return x * w - q * p;
+        uint64_t r;
+        asm("{\n\t"
+            ".reg .u32 x0, x1, v0, v1, w0, w1, h, t0, t1, s0, s1, f0, f1, q0, q1, l0, l1, qh, r0, r1;\n\t"
+            ".reg .u64 A, TT, WW, F, Q, L;\n\t"
+            "mov.b64 {x0, x1}, %1;\n\t"
+            "mov.b64 {w0, w1}, %2;\n\t"
+            "mov.b64 {v0, v1}, %3;\n\t"
+            "mul.hi.u32 h, x0, v0;\n\t"
+            "mov.b64 A, {h, 0};\n\t"
+            "mad.wide.u32 TT, x0, v1, A;\n\t"
+            "mov.b64 {t0, t1}, TT;\n\t"
+            "mov.b64 A, {t0, 0};\n\t"
+            "mad.wide.u32 WW, x1, v0, A;\n\t"
+            "mov.b64 {s0, s1}, WW;\n\t"
+            "add.cc.u32 f0, s1, t1;\n\t"
+            "addc.u32 f1, 0, 0;\n\t"
+            "mov.b64 F, {f0, f1};\n\t"
+            "mad.wide.u32 Q, x1, v1, F;\n\t"
+            "mov.b64 {q0, q1}, Q;\n\t"
+            "mul.wide.u32 L, x0, w0;\n\t"
+            "mov.b64 {l0, l1}, L;\n\t"
+            "mad.lo.u32 l1, x0, w1, l1;\n\t"
+            "mad.lo.u32 l1, x1, w0, l1;\n\t"
+            "mad.lo.u32 qh, q0, %4, q1;\n\t"
+            "sub.cc.u32 r0, l0, q0;\n\t"
+            "subc.u32 r1, l1, qh;\n\t"
+            "mov.b64 %0, {r0, r1};\n\t"
+            "}"
+            : "=l"(r)
+            : "l"(x), "l"(w), "l"(wq), "r"(c));
+        return r;
     }
     // a, b < 2p: returns a*b*2^-64 mod p in [0, 2p).  The low word of
     // t + m*p is zero by construction, so its carry is (lo != 0).
@@ -83,19 +147,86 @@ struct Ar64 {
         const uint64_t mh = __umul64hi(m, p);
         return hi + mh + (lo != 0 ? 1ull : 0ull);
     }
-    __device__ __forceinline__ void ct(T& a, T& b, T w, T wq) const {
-        const T x = red2(a);
-        const T t = shoup(b, w, wq);
-        a = x + t;
-        b = x - t + p2;
+    // x < 2^64, w < p: x*w mod p in [0, 3p) from the truncated quotient
+    // q' = x1 v1 + hi(x0 v1 + x1 v0) (the dropped x0 v0 term and the dropped
+    // low bits make q' at most 2 below hi64(x * wq)).
+    __device__ __forceinline__ T shoup3(T x, T w, T wq) const {
+        uint64_t r;
+        asm("{\n\t"
+            ".reg .u32 x0, x1, v0, v1, w0, w1, t0, t1, s0, s1, f0, f1, q0, q1, l0, l1, qh, r0, r1;\n\t"
+            ".reg .u64 A, TT, WW, F, Q, L;\n\t"
+            "mov.b64 {x0, x1}, %1;\n\t"
+            "mov.b64 {w0, w1}, %2;\n\t"
+            "mov.b64 {v0, v1}, %3;\n\t"
+            "mul.wide.u32 TT, x0, v1;\n\t"
+            "mov.b64 {t0, t1}, TT;\n\t"
+            "mov.b64 A, {t0, 0};\n\t"
+            "mad.wide.u32 WW, x1, v0, A;\n\t"
+            "mov.b64 {s0, s1}, WW;\n\t"
+            "add.cc.u32 f0, s1, t1;\n\t"
+            "addc.u32 f1, 0, 0;\n\t"
+            "mov.b64 F, {f0, f1};\n\t"
+            "mad.wide.u32 Q, x1, v1, F;\n\t"
+            "mov.b64 {q0, q1}, Q;\n\t"
+            "mul.wide.u32 L, x0, w0;\n\t"
+            "mov.b64 {l0, l1}, L;\n\t"
+            "mad.lo.u32 l1, x0, w1, l1;\n\t"
+            "mad.lo.u32 l1, x1, w0, l1;\n\t"
+            "mad.lo.u32 qh, q0, %4, q1;\n\t"
+            "sub.cc.u32 r0, l0, q0;\n\t"
+            "subc.u32 r1, l1, qh;\n\t"
+            "mov.b64 %0, {r0, r1};\n\t"
+            "}"
+            : "=l"(r)
+            : "l"(x), "l"(w), "l"(wq), "r"(c));
+        return r;
     }
+    // forward CT butterfly, inputs/outputs in [0, 6p + 2^32)
+    __device__ __forceinline__ void ct(T& a, T& b, T w, T wq) const {
+        const T x = ((uint32_t)(a >> 32) > c3) ? a - p3 : a;  // [0, 3p + 2^32)
+        const T t = shoup3(b, w, wq);                          // [0, 3p)
+        a = x + t;
+        b = x - t + p3;
+    }
+    // inverse GS butterfly, inputs/outputs in [0, 2p)
     __device__ __forceinline__ void gs(T& a, T& b, T w, T wq) const {
         const T u = a + b;
         const T v = a - b + p2;
         a = red2(u);
         b = shoup(v, w, wq);
     }
+    // twiddle-1 butterflies of stage 0 (inputs known to be in [0, 2p))
+    __device__ __forceinline__ void ct1(T& a, T& b) const {
+        const T x = a;
+        a = x + b;
+        b = x - b + p3;
+    }
+    __device__ __forceinline__ void gs1(T& a, T& b) const {
+        const T x = a;
+        a = red2(x + b);
+        b = red2(x - b + p2);
+    }
+    // forward-transform output range [0, 6p + 2^32) -> [0, 2p)
+    __device__ __forceinline__ T fwd_to_2p(T a) const { return red2(min(a, a - p4)); }
+    // Shoup companion floor(w 2^64 / p) of w < p by a Barrett step with
+    // mu = floor(2^128 / p): the estimate is at most 2 short.
+    __device__ __forceinline__ T companion(T w) const {
+        uint64_t q = w * (uint64_t)mu_hi + __umul64hi(w, mu_lo);
+        uint64_t r = 0 - q * p;
+        if (r >= p) {
+            ++q;
+            r -= p;
+        }
+        if (r >= p) ++q;
+        return q;
+    }
 };
+
+// Twiddle load from shared memory (generic pointer into the CTA's tables).
+template <typename T>
+__device__ __forceinline__ Tw<T> ld_tw_s(const Tw<T>* p) {
+    return *p;
+}
 
 template <typename T>
 __device__ __forceinline__ Tw<T> ld_tw(const Tw<T>* p) {

@@ -87,10 +87,12 @@ uint32_t bitrev_h(uint32_t x, int bits) {
 }
 
 // Primes of the two paths with a generator of the multiplicative group.
-// P64: c * 2^32 + 1 just below 2^62 (v2(p-1) = 33, 34, 37).
+// P64: c * 2^32 + 1, the largest such primes below 2^64 / 6 (62 bits,
+//      v2(p-1) = 32; the bound is what the forward butterfly's lazy range
+//      [0, 6p + 2^32) needs).
 // P32: 30-bit primes with v2(p-1) = 24, 26, 25.
-const uint64_t kP64[3] = {0x3fffffee00000001ull, 0x3fffffb400000001ull, 0x3fffffa000000001ull};
-const uint64_t kG64[3] = {3, 19, 3};
+const uint64_t kP64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
+const uint64_t kG64[3] = {10, 7, 3};
 const uint64_t kP32[3] = {754974721ull, 469762049ull, 167772161ull};
 const uint64_t kG32[3] = {11, 3, 3};
 
@@ -121,6 +123,8 @@ struct bw_plan {
     int path = 0, K = 0;
     size_t la = 0, lb = 0, nca = 0, ncb = 0;
     int log_n = 0, log_r = 0, log_c = 0, log_cb = 0, lo = 0;
+    int tw_smem_r = 0;   // column stage twiddles staged in shared memory
+    int rlog_row = 4;    // radix of the row kernel's rounds (2^3 or 2^4)
     int device = 0;
     bool zt_a = false, zt_b = false;
     void* d_tables = nullptr;
@@ -167,6 +171,17 @@ struct TableBuilder {
     }
 };
 
+inline void set_c(Ar32&, uint64_t) {}
+inline void set_c(Ar64& a, uint64_t p) {
+    a.c = (uint32_t)(p >> 32);
+    a.c3 = 3u * a.c;
+    a.p3 = 3 * p;
+    a.p4 = 4 * p;
+    const u128 mu = (~(u128)0) / p;  // floor(2^128 / p): p is odd
+    a.mu_lo = (uint64_t)mu;
+    a.mu_hi = (uint32_t)(mu >> 64);
+}
+
 template <class Ar>
 int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     using T = typename Ar::T;
@@ -210,6 +225,7 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
         pr.ar.p = (T)P[k];
         pr.ar.p2 = (T)(2 * P[k]);
         pr.ar.pinv = (T)neg_inv_pow2(P[k], bits);
+        set_c(pr.ar, P[k]);
         pr.one_q = (T)shoup_pre(1, P[k], bits);
     }
     // unused prime slots get harmless arithmetic constants
@@ -229,6 +245,8 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     pd.log_c = pl->log_c;
     pd.lo = pl->lo;
     pd.log_cb = pl->log_cb;
+    pd.tw_smem_r = pl->tw_smem_r;
+    pd.log_fa = pl->log_c / 2;
     return BW_OK;
 }
 
@@ -276,7 +294,6 @@ static int choose_path(size_t la, size_t lb) {
 
 extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int num_primes,
                               unsigned flags) {
-    (void)flags;
     bw_clear_error();
     if (!out) return bw_fail(BW_EINVAL, "out is NULL");
     *out = nullptr;
@@ -297,11 +314,23 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     const int w = path == BW_PATH_P64 ? 8 : 4;
     const int max_c = path == BW_PATH_P64 ? 13 : 14;
     pl->log_c = std::min(max_c, (log_n + 1) / 2);
+    const int want_c = (int)((flags >> 8) & 0x1f);
+    if (want_c) {
+        if (want_c > max_c || want_c >= log_n || log_n - want_c > 13) {
+            delete pl;
+            return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c, log_n);
+        }
+        pl->log_c = want_c;
+    }
     pl->log_r = log_n - pl->log_c;
     // column tile: 64 KiB of residues per shared-memory buffer
     int log_cb = 0;
     while (log_cb < pl->log_c && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536) ++log_cb;
     pl->log_cb = log_cb;
+    // stage the R-point twiddles in shared memory when they take <= 32 KiB
+    pl->tw_smem_r = ((size_t)2 * w << pl->log_r) <= 32768 ? 1 : 0;
+    if (flags & BW_PLAN_TW_GLOBAL) pl->tw_smem_r = 0;
+    pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
     pl->lo = (log_n + 1) / 2;
     const size_t half = ((size_t)1 << log_n) / 2;
     pl->zt_a = pl->nca <= half;
@@ -498,19 +527,40 @@ int set_smem_attrs() {
     static std::once_flag once;
     static cudaError_t st = cudaSuccess;
     std::call_once(once, [] {
-        cudaError_t e1 = cudaFuncSetAttribute(k_fwd_col<Ar, SPLIT16>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              kMaxDynSmem);
-        cudaError_t e2 = cudaFuncSetAttribute(
-            k_row<Ar, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-        cudaError_t e3 = cudaFuncSetAttribute(
-            k_row<Ar, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-        cudaError_t e4 = cudaFuncSetAttribute(
-            k_inv_col<Ar>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-        st = e1 ? e1 : e2 ? e2 : e3 ? e3 : e4;
+        auto set = [](const void* f) {
+            cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 kMaxDynSmem);
+            if (e != cudaSuccess) st = e;
+        };
+        set((const void*)k_fwd_col<Ar, SPLIT16, 4, true>);
+        set((const void*)k_fwd_col<Ar, SPLIT16, 4, false>);
+        set((const void*)k_inv_col<Ar, 4, true>);
+        set((const void*)k_inv_col<Ar, 4, false>);
+        set((const void*)k_row<Ar, 64, 4>);
+        set((const void*)k_row<Ar, 128, 4>);
+        set((const void*)k_row<Ar, 256, 4>);
+        set((const void*)k_row<Ar, 512, 4>);
+        set((const void*)k_row<Ar, 64, 3>);
+        set((const void*)k_row<Ar, 128, 3>);
+        set((const void*)k_row<Ar, 256, 3>);
+        set((const void*)k_row<Ar, 512, 3>);
     });
     if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
     return BW_OK;
+}
+
+template <class Ar, int RLOG>
+void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
+                const typename Ar::T* rb, int sq, size_t smem, cudaStream_t s) {
+    dim3 g(1u << pl->log_r, pl->K);
+    // one thread per sub-problem of a round, 64..512 threads
+    const int want = std::min(512, std::max(64, 1 << (pl->log_c - RLOG)));
+    switch (want) {
+        case 512: k_row<Ar, 512, RLOG><<<g, 512, smem, s>>>(pd, ra, rb, sq); break;
+        case 256: k_row<Ar, 256, RLOG><<<g, 256, smem, s>>>(pd, ra, rb, sq); break;
+        case 128: k_row<Ar, 128, RLOG><<<g, 128, smem, s>>>(pd, ra, rb, sq); break;
+        default: k_row<Ar, 64, RLOG><<<g, 64, smem, s>>>(pd, ra, rb, sq); break;
+    }
 }
 
 // Enqueue K1..K3 (the transform part) for one product.
@@ -525,26 +575,40 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const int R = 1 << pl->log_r, C = 1 << pl->log_c, CB = 1 << pl->log_cb;
     T* ra = reinterpret_cast<T*>(c->d_res_a);
     T* rb = reinterpret_cast<T*>(c->d_res_b);
+    const bool ts = pl->tw_smem_r != 0;
+    const size_t tw_bytes = ts ? (size_t)R * sizeof(Tw<T>) : 0;
 
-    const size_t smem1 = (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
+    const size_t smem1 = tw_bytes + (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
     dim3 g1(C / CB, 1, square ? 1 : 2);
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
-    k_fwd_col<Ar, SPLIT16><<<g1, kColThreads, smem1, c->stream>>>(pd, a, pl->nca, b, pl->ncb,
-                                                                  ra, rb, zt);
+    if (ts) {
+        k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(
+            pd, a, pl->nca, b, pl->ncb, ra, rb, zt);
+    } else {
+        k_fwd_col<Ar, SPLIT16, 4, false><<<g1, kColThreads, smem1, c->stream>>>(
+            pd, a, pl->nca, b, pl->ncb, ra, rb, zt);
+    }
     if (timing) cudaEventRecord(c->ev[2], c->stream);
 
-    const size_t smem2 = (size_t)C * sizeof(T) * (square ? 1 : 2);
-    dim3 g2(R, pl->K);
-    if (pl->log_c >= 12) {
-        k_row<Ar, 512><<<g2, 512, smem2, c->stream>>>(pd, ra, square ? ra : rb, square ? 1 : 0);
+    const int la = pl->log_c / 2;
+    const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
+    const size_t smem2 = ntab * sizeof(Tw<T>) + (size_t)C * sizeof(T) * (square ? 1 : 2);
+    const T* rbs = square ? ra : rb;
+    const int sq = square ? 1 : 0;
+    if (pl->rlog_row == 3) {
+        launch_row<Ar, 3>(pl, pd, ra, rbs, sq, smem2, c->stream);
     } else {
-        k_row<Ar, 256><<<g2, 256, smem2, c->stream>>>(pd, ra, square ? ra : rb, square ? 1 : 0);
+        launch_row<Ar, 4>(pl, pd, ra, rbs, sq, smem2, c->stream);
     }
     if (timing) cudaEventRecord(c->ev[3], c->stream);
 
-    const size_t smem3 = (size_t)R * CB * sizeof(T);
+    const size_t smem3 = tw_bytes + (size_t)R * CB * sizeof(T);
     dim3 g3(C / CB, pl->K);
-    k_inv_col<Ar><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+    if (ts) {
+        k_inv_col<Ar, 4, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+    } else {
+        k_inv_col<Ar, 4, false><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+    }
     if (timing) cudaEventRecord(c->ev[4], c->stream);
     BW_CUDA(cudaGetLastError());
     return BW_OK;

@@ -1,14 +1,15 @@
 // bw_kernels.cuh -- device side of the product pipeline (both prime paths).
 //
 // A product of two operands is computed as a cyclic convolution of length
-// n = 2^log_n = R * C per prime with a 4-step NTT:
+// n = 2^log_n = R * C per prime with a 4-step NTT (R rows, C columns,
+// element (r, c) = coefficient r*C + c):
 //
-//   K1 fwd_col   per operand, per tile of CB columns of the R x C matrix:
-//                limb split + virtual zero pad, R-point forward NTT down each
-//                column, inter-pass twiddle w_n^(c * bitrev(r)), write.
-//   K2 row       per prime, per row: C-point forward NTT of the A row and the
+//   K1 fwd_col   per operand, per tile of CB columns: limb split + virtual
+//                zero pad, R-point forward NTT down each column, write.
+//   K2 row       per prime, per row p (k1 = bitrev(p)): inter-pass twiddle
+//                w_n^(c k1) on load, C-point forward NTT of the A row and the
 //                B row, pointwise Montgomery product, C-point inverse NTT,
-//                inverse twiddle (scaled by n^-1 * 2^bits), write in place.
+//                inverse twiddle w_n^(-c k1) n^-1 2^bits, write in place.
 //   K3 inv_col   per prime, per column tile: R-point inverse NTT down each
 //                column, full reduction, write residues in natural order.
 //   K4 garner_carry  per tile of 2048 output words: Garner reconstruction of
@@ -16,11 +17,15 @@
 //                carry propagation across tiles by decoupled look-back.
 //
 // Forward transforms are Cooley-Tukey with natural-order input and
-// bit-reversed output ("CT-BR"); inverse transforms are Gentleman-Sande with
+// bit-reversed output; inverse transforms are Gentleman-Sande with
 // bit-reversed input and natural output.  Stage s (m = 2^s groups) uses the
 // twiddle table entries W[m .. 2m), W[m + i] = w_{2m}^{bitrev_s(i)}.  Each
-// round processes up to four stages in registers (radix 16); rounds exchange
-// data through swizzled shared memory.
+// round processes up to 2^RLOG elements per thread in registers (radix 8 or
+// 16); rounds exchange data through swizzled shared memory.  Stage twiddle
+// tables are staged in shared memory when they fit.  The inter-pass twiddle
+// of a row is split as w_n^(c k1) = F[c mod 2^a] G[c >> a] with per-row
+// tables F, G (about 2 sqrt(C) entries) built in shared memory at the start
+// of K2, their Shoup companions computed on the device.
 //
 // The reference runs these stages as separate kernels with separate HBM
 // passes: zero_pad (src/zero_pad.cu:3-57), GPU-NTT forward/inverse
@@ -47,10 +52,10 @@ struct PrimeDev {
     const Tw<T>* WRi;  // column inverse
     const Tw<T>* WCf;  // row (C-point) forward, C entries
     const Tw<T>* WCi;  // row inverse
-    const Tw<T>* TLf;  // inter-pass twiddle w_n^e, e = eh*2^LO + el: low table
-    const Tw<T>* THf;  //   high table
-    const Tw<T>* TLi;  // inverse inter-pass twiddle, low table
-    const Tw<T>* THi;  //   high table, scaled by n^-1 * 2^bits
+    const Tw<T>* TLf;  // w_n^e for e < 2^lo
+    const Tw<T>* THf;  // w_n^(e 2^lo) for e < n / 2^lo
+    const Tw<T>* TLi;  // w_n^-e
+    const Tw<T>* THi;  // w_n^-(e 2^lo) * n^-1 * 2^bits
     Ar ar;
     T one_q;           // floor(2^bits / p): Shoup companion of 1 (x mod p)
 };
@@ -73,6 +78,8 @@ struct PlanDev {
     int K;
     int log_n, log_r, log_c, lo;  // lo: split of the inter-pass exponent
     int log_cb;                   // column tile width CB = 2^log_cb
+    int tw_smem_r;                // stage the R-point twiddles in shared memory
+    int log_fa;                   // per-row twiddle split a (F has 2^a entries)
 };
 
 // Carry look-back state of one context.
@@ -113,39 +120,41 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Round schedule of a 2^log_len-point transform: the remainder round (fewer
-// than four stages) comes first, where the sub-problem stride is largest and
-// shared-memory accesses are conflict-free; all later rounds are radix 16.
-struct Sched {
-    int n;
-    int s0[8];
-    int rl[8];
-};
-__host__ __device__ __forceinline__ Sched make_sched(int log_len) {
-    Sched s;
-    s.n = 0;
-    int at = 0;
-    const int rem = log_len & 3;
-    if (rem) {
-        s.s0[0] = 0;
-        s.rl[0] = rem;
-        s.n = 1;
-        at = rem;
+// Round schedule of a 2^log_len-point transform with rounds of up to RLOG
+// stages: the remainder round comes first, where the sub-problem stride is
+// largest and shared-memory accesses are conflict-free.  Computed
+// arithmetically (no arrays, so nothing goes to local memory).
+template <int RLOG>
+__host__ __device__ __forceinline__ int sched_rounds(int log_len) {
+    return (log_len + RLOG - 1) / RLOG;
+}
+template <int RLOG>
+__host__ __device__ __forceinline__ int sched_rl(int log_len, int r) {
+    const int rem = log_len % RLOG;
+    return (rem && r == 0) ? rem : RLOG;
+}
+template <int RLOG>
+__host__ __device__ __forceinline__ int sched_s0(int log_len, int r) {
+    const int rem = log_len % RLOG;
+    return rem ? (r == 0 ? 0 : rem + RLOG * (r - 1)) : RLOG * r;
+}
+
+// Twiddle load from shared (TS) or global memory.
+template <bool TS, typename T>
+__device__ __forceinline__ Tw<T> ld_w(const Tw<T>* p) {
+    if constexpr (TS) {
+        return *p;
+    } else {
+        return ld_tw(p);
     }
-    while (at < log_len) {
-        s.s0[s.n] = at;
-        s.rl[s.n] = 4;
-        s.n++;
-        at += 4;
-    }
-    return s;
 }
 
 // Forward CT stages s0 .. s0+RL-1 on one sub-problem of 2^RL elements that
-// belongs to group g of stage s0.  With zt (first round of a zero-padded
-// column) the elements of the second half are zero and stage 0 (twiddle 1)
-// reduces to duplicating the first half.
-template <class Ar, int RL>
+// belongs to group g of stage s0.  In the first round of a transform (s0 = 0)
+// stage 0 has twiddle 1 and inputs in [0, 2p), so its butterflies need no
+// multiply; with zt (first round of a zero-padded column) the second half is
+// zero and stage 0 just duplicates the first half.
+template <class Ar, int RL, bool TS>
 __device__ __forceinline__ void ct_stages(typename Ar::T* x, int s0, int g,
                                           const Tw<typename Ar::T>* __restrict__ W,
                                           const Ar& ar, bool zt) {
@@ -153,15 +162,20 @@ __device__ __forceinline__ void ct_stages(typename Ar::T* x, int s0, int g,
 #pragma unroll
     for (int l = 0; l < RL; ++l) {
         const int h = 1 << (RL - l - 1);
-        if (l == 0 && zt) {
+        if (l == 0 && s0 == 0) {
+            if (zt) {
 #pragma unroll
-            for (int u = 0; u < h; ++u) x[u + h] = x[u];
+                for (int u = 0; u < h; ++u) x[u + h] = x[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < h; ++u) ar.ct1(x[u], x[u + h]);
+            }
             continue;
         }
         const Tw<T>* Ws = W + (1 << (s0 + l)) + (g << l);
 #pragma unroll
         for (int q = 0; q < (1 << l); ++q) {
-            const Tw<T> w = ld_tw(Ws + q);
+            const Tw<T> w = ld_w<TS>(Ws + q);
 #pragma unroll
             for (int u = 0; u < h; ++u) {
                 const int k = (q << (RL - l)) + u;
@@ -171,8 +185,9 @@ __device__ __forceinline__ void ct_stages(typename Ar::T* x, int s0, int g,
     }
 }
 
-// Inverse GS stages s0+RL-1 down to s0 (the mirror of ct_stages).
-template <class Ar, int RL>
+// Inverse GS stages s0+RL-1 down to s0 (the mirror of ct_stages); stage 0
+// has twiddle 1.
+template <class Ar, int RL, bool TS>
 __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
                                           const Tw<typename Ar::T>* __restrict__ W,
                                           const Ar& ar) {
@@ -180,10 +195,15 @@ __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
 #pragma unroll
     for (int l = RL - 1; l >= 0; --l) {
         const int h = 1 << (RL - l - 1);
+        if (l == 0 && s0 == 0) {
+#pragma unroll
+            for (int u = 0; u < h; ++u) ar.gs1(x[u], x[u + h]);
+            continue;
+        }
         const Tw<T>* Ws = W + (1 << (s0 + l)) + (g << l);
 #pragma unroll
         for (int q = 0; q < (1 << l); ++q) {
-            const Tw<T> w = ld_tw(Ws + q);
+            const Tw<T> w = ld_w<TS>(Ws + q);
 #pragma unroll
             for (int u = 0; u < h; ++u) {
                 const int k = (q << (RL - l)) + u;
@@ -194,8 +214,8 @@ __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
 }
 
 // One round over all sub-problems of a batch of 2^log_cb vectors of length
-// 2^log_len.  ld(v, idx, k) / st(v, idx, val) move element idx of vector v.
-template <class Ar, int RL, bool INV, class LD, class ST>
+// 2^log_len.  ld(v, idx) / st(v, idx, val) move element idx of vector v.
+template <class Ar, int RL, bool INV, bool TS, class LD, class ST>
 __device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
                                           const Tw<typename Ar::T>* __restrict__ W,
                                           const Ar& ar, bool zt, LD ld, ST st) {
@@ -210,37 +230,39 @@ __device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
         const int base = (g << (d_log + RL)) + j;
         T x[1 << RL];
 #pragma unroll
-        for (int k = 0; k < (1 << RL); ++k) x[k] = ld(v, base + (k << d_log), k);
+        for (int k = 0; k < (1 << RL); ++k) x[k] = ld(v, base + (k << d_log));
         if constexpr (!INV) {
-            ct_stages<Ar, RL>(x, s0, g, W, ar, zt);
+            ct_stages<Ar, RL, TS>(x, s0, g, W, ar, zt);
         } else {
-            gs_stages<Ar, RL>(x, s0, g, W, ar);
+            gs_stages<Ar, RL, TS>(x, s0, g, W, ar);
         }
 #pragma unroll
         for (int k = 0; k < (1 << RL); ++k) st(v, base + (k << d_log), x[k]);
     }
 }
 
-template <class Ar, bool INV, class LD, class ST>
+// Dispatch on the round's radix: only the remainder round (the first round of
+// a transform) is narrower than 2^RLOG, so the full radix has one
+// instantiation per call site and the narrow ones stay small.
+template <class Ar, int RLOG, bool INV, bool TS, class LD, class ST>
 __device__ __forceinline__ void run_round_rl(int rl, int log_len, int log_cb, int s0,
                                              const Tw<typename Ar::T>* __restrict__ W,
                                              const Ar& ar, bool zt, LD ld, ST st) {
-    switch (rl) {
-        case 1: run_round<Ar, 1, INV>(log_len, log_cb, s0, W, ar, zt, ld, st); break;
-        case 2: run_round<Ar, 2, INV>(log_len, log_cb, s0, W, ar, zt, ld, st); break;
-        case 3: run_round<Ar, 3, INV>(log_len, log_cb, s0, W, ar, zt, ld, st); break;
-        default: run_round<Ar, 4, INV>(log_len, log_cb, s0, W, ar, zt, ld, st); break;
+    if (rl == RLOG) {
+        run_round<Ar, RLOG, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+    } else if (rl == 3) {
+        run_round<Ar, 3, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+    } else if (rl == 2) {
+        run_round<Ar, 2, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+    } else {
+        run_round<Ar, 1, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
     }
 }
 
-// Apply a two-level inter-pass twiddle w^e = TL[e mod 2^lo] * TH[e >> lo].
-template <class Ar>
-__device__ __forceinline__ typename Ar::T twiddle2(const Ar& ar, typename Ar::T x, uint32_t e,
-                                                   int lo, const Tw<typename Ar::T>* TL,
-                                                   const Tw<typename Ar::T>* TH) {
-    const auto a = ld_tw(TL + (e & ((1u << lo) - 1)));
-    const auto b = ld_tw(TH + (e >> lo));
-    return ar.shoup(ar.shoup(x, a.w, a.wq), b.w, b.wq);
+// Copy a stage twiddle table (2^log_len entries) into shared memory.
+template <typename T>
+__device__ __forceinline__ void stage_table(Tw<T>* dst, const Tw<T>* src, int log_len) {
+    for (int i = threadIdx.x; i < (1 << log_len); i += blockDim.x) dst[i] = ld_tw(src + i);
 }
 
 // ------------------------------------------------------------------ K1
@@ -249,7 +271,7 @@ __device__ __forceinline__ typename Ar::T twiddle2(const Ar& ar, typename Ar::T 
 // coefficients.  ncoef = number of coefficients of the operand; the column
 // tail beyond it is the virtual zero pad.  zt_mask bit z says operand z has
 // all coefficients in the top half of the rows (rows >= R/2 are zero).
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, int RLOG, bool TS>
 __global__ void __launch_bounds__(kColThreads)
 k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
           const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
@@ -268,7 +290,8 @@ k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoe
     const int c0 = blockIdx.x << log_cb;
     const int rows_loaded = zt ? R / 2 : R;
 
-    T* buf = reinterpret_cast<T*>(smem_raw);
+    Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
+    T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
     uint32_t* coef = reinterpret_cast<uint32_t*>(buf + (R << log_cb));
 
     for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
@@ -283,45 +306,65 @@ k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoe
         }
         coef[e] = val;
     }
-    __syncthreads();
 
-    const Sched sc = make_sched(log_r);
+    const int nr = sched_rounds<RLOG>(log_r);
     for (int kp = 0; kp < P.K; ++kp) {
         const PrimeDev<Ar>& pr = P.pr[kp];
         const Ar ar = pr.ar;
         T* gout = res + (size_t)kp * n;
-        for (int r = 0; r < sc.n; ++r) {
-            const bool first = (r == 0), last = (r == sc.n - 1);
-            auto ld_coef = [&](int v, int idx, int k) -> T {
-                if (zt && k >= 0 && idx >= R / 2) return T(0);
-                return (T)coef[(idx << log_cb) + v];
+        const Tw<T>* W = pr.WRf;
+        if constexpr (TS) {
+            if (kp > 0) __syncthreads();
+            stage_table(tws, pr.WRf, log_r);
+            W = tws;
+        }
+        __syncthreads();
+        for (int r = 0; r < nr; ++r) {
+            const bool first = (r == 0), last = (r == nr - 1);
+            // first round reads the coefficient tile (zero pad virtual), last
+            // round writes to global memory
+            auto ld = [&](int v, int idx) -> T {
+                if (first) {
+                    if (zt && idx >= R / 2) return T(0);
+                    return (T)coef[(idx << log_cb) + v];
+                }
+                return buf[swz<T>((idx << log_cb) + v)];
             };
-            auto ld_smem = [&](int v, int idx, int) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
-            auto st_smem = [&](int v, int idx, T val) { buf[swz<T>((idx << log_cb) + v)] = val; };
-            auto st_glob = [&](int v, int idx, T val) {
-                const uint32_t c = (uint32_t)(c0 + v);
-                const uint32_t e = c * bitrev((uint32_t)idx, log_r);
-                gout[(size_t)idx * C + c] = twiddle2(ar, val, e, P.lo, pr.TLf, pr.THf);
+            auto st = [&](int v, int idx, T val) {
+                if (last) {
+                    gout[(size_t)idx * C + c0 + v] = val;
+                } else {
+                    buf[swz<T>((idx << log_cb) + v)] = val;
+                }
             };
-            if (first && last) {
-                run_round_rl<Ar, false>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRf, ar, zt, ld_coef, st_glob);
-            } else if (first) {
-                run_round_rl<Ar, false>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRf, ar, zt, ld_coef, st_smem);
-            } else if (last) {
-                run_round_rl<Ar, false>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRf, ar, false, ld_smem, st_glob);
-            } else {
-                run_round_rl<Ar, false>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRf, ar, false, ld_smem, st_smem);
-            }
+            run_round_rl<Ar, RLOG, false, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
+                                              sched_s0<RLOG>(log_r, r), W, ar, first && zt, ld,
+                                              st);
             __syncthreads();
         }
     }
 }
 
 // ------------------------------------------------------------------ K2
-// Fused row pass for row blockIdx.x and prime blockIdx.y: forward C-point NTT
-// of both rows, pointwise product, inverse C-point NTT, inverse twiddle.
-// The result overwrites the A row.  square: B is A.
-template <class Ar, int NT>
+// Per-row twiddle tables: F[i] = w^(i k1), G[j] = w^(j 2^a k1) (forward) and
+// the inverse pair with n^-1 2^bits folded into Gi.  w^e comes from the
+// plan's two-level tables; each entry's Shoup companion is computed here.
+template <class Ar>
+__device__ __forceinline__ Tw<typename Ar::T> pow_entry(const Ar& ar, uint64_t e, int lo,
+                                                        const Tw<typename Ar::T>* TL,
+                                                        const Tw<typename Ar::T>* TH) {
+    using T = typename Ar::T;
+    const auto a = ld_tw(TL + (e & ((1ull << lo) - 1)));
+    const auto b = ld_tw(TH + (e >> lo));
+    const T w = ar.red1(ar.shoup(a.w, b.w, b.wq));
+    return Tw<T>{w, ar.companion(w)};
+}
+
+// Fused row pass for row blockIdx.x and prime blockIdx.y: inter-pass twiddle
+// on load, forward C-point NTT of both rows, pointwise product, inverse
+// C-point NTT, inverse twiddle.  The result overwrites the A row.
+// square: B is A.
+template <class Ar, int NT, int RLOG>
 __global__ void __launch_bounds__(NT)
 k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, int square) {
     using T = typename Ar::T;
@@ -335,35 +378,57 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
     const Ar ar = pr.ar;
     T* ga = res_a + (size_t)kp * n + (size_t)prow * C;
     const T* gb = res_b + (size_t)kp * n + (size_t)prow * C;
-    T* bufA = reinterpret_cast<T*>(smem_raw);
+    const int la = P.log_fa, nf = 1 << la, ng = C >> la;
+    Tw<T>* F = reinterpret_cast<Tw<T>*>(smem_raw);
+    Tw<T>* G = F + nf;
+    Tw<T>* Fi = G + ng;
+    Tw<T>* Gi = Fi + nf;
+    T* bufA = reinterpret_cast<T*>(Gi + ng);
     T* bufB = bufA + C;
 
-    for (int i = threadIdx.x; i < C; i += NT) {
-        bufA[swz<T>(i)] = ga[i];
-        if (!square) bufB[swz<T>(i)] = gb[i];
+    const uint64_t k1 = bitrev((uint32_t)prow, log_r);
+    const uint64_t nmask = n - 1;
+    // F[i] = w^(i k1), G[j] = w^(j 2^a k1), Fi[i] = w^(-i k1) (forward tables
+    // at exponent n - e), Gi[j] = w^(-j 2^a k1) n^-1 2^bits (inverse tables,
+    // whose high table carries the scale)
+    for (int i = threadIdx.x; i < nf + ng; i += NT) {
+        if (i < nf) {
+            const uint64_t e = ((uint64_t)i * k1) & nmask;
+            F[i] = pow_entry(ar, e, P.lo, pr.TLf, pr.THf);
+            Fi[i] = pow_entry(ar, (n - e) & nmask, P.lo, pr.TLf, pr.THf);
+        } else {
+            const uint64_t e = (((uint64_t)(i - nf) << la) * k1) & nmask;
+            G[i - nf] = pow_entry(ar, e, P.lo, pr.TLf, pr.THf);
+            Gi[i - nf] = pow_entry(ar, e, P.lo, pr.TLi, pr.THi);
+        }
     }
     __syncthreads();
 
-    const Sched sc = make_sched(log_c);
-    auto ldA = [&](int, int idx, int) -> T { return bufA[swz<T>(idx)]; };
-    auto stA = [&](int, int idx, T v) { bufA[swz<T>(idx)] = v; };
-    auto ldB = [&](int, int idx, int) -> T { return bufB[swz<T>(idx)]; };
-    auto stB = [&](int, int idx, T v) { bufB[swz<T>(idx)] = v; };
-    const uint32_t k1 = bitrev((uint32_t)prow, log_r);
-    auto st_glob = [&](int, int idx, T v) {
-        const uint32_t e = (uint32_t)idx * k1;
-        ga[idx] = twiddle2(ar, v, e, P.lo, pr.TLi, pr.THi);
+    for (int i = threadIdx.x; i < C; i += NT) {
+        const Tw<T> f = F[i & (nf - 1)], g = G[i >> la];
+        bufA[swz<T>(i)] = ar.shoup(ar.shoup(ga[i], f.w, f.wq), g.w, g.wq);
+        if (!square) bufB[swz<T>(i)] = ar.shoup(ar.shoup(gb[i], f.w, f.wq), g.w, g.wq);
+    }
+    __syncthreads();
+
+    const int nr = sched_rounds<RLOG>(log_c);
+    auto ldA = [&](int, int idx) -> T { return bufA[swz<T>(idx)]; };
+    auto st_glob = [&](int idx, T v) {
+        const Tw<T> f = Fi[idx & (nf - 1)], g = Gi[idx >> la];
+        ga[idx] = ar.shoup(ar.shoup(v, f.w, f.wq), g.w, g.wq);
     };
 
-    // forward rounds: A fully (all but the last when squaring), B all but the last
-    const int a_rounds = square ? sc.n - 1 : sc.n;
-    for (int r = 0; r < a_rounds; ++r) {
-        run_round_rl<Ar, false>(sc.rl[r], log_c, 0, sc.s0[r], pr.WCf, ar, false, ldA, stA);
-        __syncthreads();
-    }
-    if (!square) {
-        for (int r = 0; r < sc.n - 1; ++r) {
-            run_round_rl<Ar, false>(sc.rl[r], log_c, 0, sc.s0[r], pr.WCf, ar, false, ldB, stB);
+    // forward rounds: A fully (all but the last when squaring), B all but the
+    // last (its last round is fused with the product below)
+    for (int op = 0; op < (square ? 1 : 2); ++op) {
+        T* buf = op ? bufB : bufA;
+        const int rounds = (op == 0 && !square) ? nr : nr - 1;
+        auto ld = [&](int, int idx) -> T { return buf[swz<T>(idx)]; };
+        auto st = [&](int, int idx, T v) { buf[swz<T>(idx)] = v; };
+        for (int r = 0; r < rounds; ++r) {
+            run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
+                                                 sched_s0<RLOG>(log_c, r), pr.WCf, ar, false,
+                                                 ld, st);
             __syncthreads();
         }
     }
@@ -371,52 +436,60 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
     // fused round: last forward round of B (or A), pointwise product, first
     // inverse round -- one sub-problem stays in registers throughout.
     {
-        const int r = sc.n - 1;
-        const int rl = sc.rl[r], s0 = sc.s0[r];
+        const int r = nr - 1;
+        const int rl = sched_rl<RLOG>(log_c, r), s0 = sched_s0<RLOG>(log_c, r);
         const int d_log = log_c - s0 - rl;
         const int nsub = 1 << (log_c - rl);
-        const bool final_round = (sc.n == 1);
+        const bool final_round = (nr == 1);
         T* src = square ? bufA : bufB;
         for (int sp = threadIdx.x; sp < nsub; sp += NT) {
             const int j = sp & ((1 << d_log) - 1);
             const int g = sp >> d_log;
             const int base = (g << (d_log + rl)) + j;
-            T x[16];
+            T x[1 << RLOG];
 #define BW_FUSED_BODY(RL)                                                              \
     {                                                                                  \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] =                   \
             src[swz<T>(base + (k << d_log))];                                          \
-        ct_stages<Ar, RL>(x, s0, g, pr.WCf, ar, false);                                \
+        ct_stages<Ar, RL, false>(x, s0, g, pr.WCf, ar, false);                         \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
-            const T xa = ar.red2(x[k]);                                                \
-            const T ya = square ? xa : ar.red2(bufA[swz<T>(base + (k << d_log))]);     \
+            const T xa = ar.fwd_to_2p(x[k]);                                           \
+            const T ya = square ? xa : ar.fwd_to_2p(bufA[swz<T>(base + (k << d_log))]); \
             x[k] = ar.mont(xa, ya);                                                    \
         }                                                                              \
-        gs_stages<Ar, RL>(x, s0, g, pr.WCi, ar);                                       \
+        gs_stages<Ar, RL, false>(x, s0, g, pr.WCi, ar);                                \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
             const int idx = base + (k << d_log);                                       \
-            if (final_round) st_glob(0, idx, x[k]); else bufA[swz<T>(idx)] = x[k];     \
+            if (final_round) st_glob(idx, x[k]); else bufA[swz<T>(idx)] = x[k];        \
         }                                                                              \
     }
-            switch (rl) {
-                case 1: BW_FUSED_BODY(1) break;
-                case 2: BW_FUSED_BODY(2) break;
-                case 3: BW_FUSED_BODY(3) break;
-                default: BW_FUSED_BODY(4) break;
+            if (rl == RLOG) {
+                BW_FUSED_BODY(RLOG)
+            } else if (rl == 3) {
+                BW_FUSED_BODY(3)
+            } else if (rl == 2) {
+                BW_FUSED_BODY(2)
+            } else {
+                BW_FUSED_BODY(1)
             }
 #undef BW_FUSED_BODY
         }
         __syncthreads();
     }
 
-    // remaining inverse rounds, last one writes to global with the twiddle
-    for (int r = sc.n - 2; r >= 0; --r) {
-        if (r == 0) {
-            run_round_rl<Ar, true>(sc.rl[r], log_c, 0, sc.s0[r], pr.WCi, ar, false, ldA, st_glob);
-        } else {
-            run_round_rl<Ar, true>(sc.rl[r], log_c, 0, sc.s0[r], pr.WCi, ar, false, ldA, stA);
-            __syncthreads();
-        }
+    // remaining inverse rounds, the last one writes to global with the twiddle
+    for (int r = nr - 2; r >= 0; --r) {
+        const bool last = (r == 0);
+        auto st = [&](int, int idx, T v) {
+            if (last) {
+                st_glob(idx, v);
+            } else {
+                bufA[swz<T>(idx)] = v;
+            }
+        };
+        run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
+                                            sched_s0<RLOG>(log_c, r), pr.WCi, ar, false, ldA, st);
+        __syncthreads();
     }
 }
 
@@ -424,7 +497,7 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
 // Inverse column pass for prime blockIdx.y, column tile blockIdx.x.  Writes
 // fully reduced residues of the cyclic convolution in natural order, in place.
 // Block (0,0) also resets the carry ticket for the K4 launch that follows.
-template <class Ar>
+template <class Ar, int RLOG, bool TS>
 __global__ void __launch_bounds__(kColThreads)
 k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
     using T = typename Ar::T;
@@ -439,25 +512,32 @@ k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
     const PrimeDev<Ar>& pr = P.pr[kp];
     const Ar ar = pr.ar;
     T* g = res + (size_t)kp * n;
-    T* buf = reinterpret_cast<T*>(smem_raw);
+    Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);
+    T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
+    const Tw<T>* W = pr.WRi;
+    if constexpr (TS) {
+        stage_table(tws, pr.WRi, log_r);
+        W = tws;
+        __syncthreads();
+    }
 
-    auto ld_glob = [&](int v, int idx, int) -> T { return g[(size_t)idx * C + c0 + v]; };
-    auto st_glob = [&](int v, int idx, T val) { g[(size_t)idx * C + c0 + v] = ar.red1(val); };
-    auto ld_smem = [&](int v, int idx, int) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
-    auto st_smem = [&](int v, int idx, T val) { buf[swz<T>((idx << log_cb) + v)] = val; };
-
-    const Sched sc = make_sched(log_r);
-    for (int r = sc.n - 1; r >= 0; --r) {
-        const bool first = (r == sc.n - 1), last = (r == 0);
-        if (first && last) {
-            run_round_rl<Ar, true>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRi, ar, false, ld_glob, st_glob);
-        } else if (first) {
-            run_round_rl<Ar, true>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRi, ar, false, ld_glob, st_smem);
-        } else if (last) {
-            run_round_rl<Ar, true>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRi, ar, false, ld_smem, st_glob);
-        } else {
-            run_round_rl<Ar, true>(sc.rl[r], log_r, log_cb, sc.s0[r], pr.WRi, ar, false, ld_smem, st_smem);
-        }
+    const int nr = sched_rounds<RLOG>(log_r);
+    for (int r = nr - 1; r >= 0; --r) {
+        const bool first = (r == nr - 1), last = (r == 0);
+        // first round reads global memory, last round reduces and writes it
+        auto ld = [&](int v, int idx) -> T {
+            if (first) return g[(size_t)idx * C + c0 + v];
+            return buf[swz<T>((idx << log_cb) + v)];
+        };
+        auto st = [&](int v, int idx, T val) {
+            if (last) {
+                g[(size_t)idx * C + c0 + v] = ar.red1(val);
+            } else {
+                buf[swz<T>((idx << log_cb) + v)] = val;
+            }
+        };
+        run_round_rl<Ar, RLOG, true, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
+                                         sched_s0<RLOG>(log_r, r), W, ar, false, ld, st);
         __syncthreads();
     }
 }

@@ -70,6 +70,15 @@ extern "C" {
 #define BW_PATH_P32    32
 #define BW_PATH_P64    64
 
+/* ---- flags for bw_plan_create --------------------------------------------- */
+/* Split the transform into rows x 2^x columns for the 4-step schedule
+ * (0 = automatic).  x <= 13 (64-bit path) or 14 (32-bit path). */
+#define BW_PLAN_LOG_COLS(x) (((unsigned)(x) & 0x1fu) << 8)
+/* Tuning switches: radix-8 instead of radix-16 rounds in the row pass; keep
+ * the column stage twiddles in global memory instead of shared memory. */
+#define BW_PLAN_RADIX8     (1u << 16)
+#define BW_PLAN_TW_GLOBAL  (1u << 17)
+
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
                                 the call copies in, computes, copies out and

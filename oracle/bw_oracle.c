@@ -398,8 +398,8 @@ done:
 
 /* The library's two bases (same primes as libbirdwing), roots derived from a
  * generator of the multiplicative group. */
-static const uint64_t P64[3] = {0x3fffffee00000001ull, 0x3fffffb400000001ull, 0x3fffffa000000001ull};
-static const uint64_t G64[3] = {3, 19, 3};
+static const uint64_t P64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
+static const uint64_t G64[3] = {10, 7, 3};
 static const uint64_t P32[3] = {754974721ull, 469762049ull, 167772161ull};
 static const uint64_t G32[3] = {11, 3, 3};
 

@@ -31,8 +31,8 @@ def test_full_mul_py_golden():
 
 
 def test_ntt_roundtrip_and_definition():
-    p = 0x3fffffee00000001
     primes, roots, logs = oracle.path_basis(64)
+    p = primes[0]
     w = oracle.lib.oracle_root_for(primes[0], roots[0], logs[0], 4)
     x = list(range(1, 17))
     X = oracle.ntt(x, w, p)
