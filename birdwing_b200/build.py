@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbirdwing.so")
-SOURCES = ["bw_core.cu"]
+SOURCES = ["bw_core.cu", "bw_noalloc.cu"]
 HEADERS = ["bw_arith.cuh", "bw_kernels.cuh", "bw_host.h"]
 
 NVCC_FLAGS = [

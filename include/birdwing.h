@@ -194,6 +194,35 @@ int bw_multiply_coeffs(bw_ctx* ctx, const uint32_t* a, size_t la,
 int bw_ctx_set_wait_limit(bw_ctx* ctx, int polls);
 int bw_ctx_inject_wait_fault(bw_ctx* ctx, int enable);
 
+/* Largest number of 2048-word carry tiles bw_garner_carry_noalloc handles:
+ * up to 2^26 output words (products of up to 2^31 bits). */
+#define BW_NOALLOC_MAX_TILES 32768
+
+/* Garner reconstruction + carry propagation of a finished cyclic
+ * convolution, for callers that must not allocate device memory: cudaMalloc
+ * and cudaFree can synchronise the whole device, are not allowed while a
+ * stream is being captured into a CUDA graph, and some programs hand all
+ * device memory to their own pool allocator.  This call allocates nothing.
+ * The caller passes residues (device memory, 16-byte aligned): num_primes
+ * arrays of n fully reduced residues, array k at residues + k * n elements,
+ * u64 elements for BW_PATH_P64 and u32 for BW_PATH_P32, in natural
+ * coefficient order, exactly as the library's own pipeline leaves them.  It
+ * writes out[0 .. min(out_words, n / c)) with c = 1 (P64) or 2 (P32: two
+ * 16-bit coefficients per word).  The primes are the library's, see
+ * bw_plan_get_info.  n is a power of two >= 16 and n / c is at most
+ * BW_NOALLOC_MAX_TILES * 2048, else BW_ESIZE.  The look-back scratch is one
+ * fixed-size device array in the library (about 640 KiB on every GPU that
+ * loads it, kept until exit); every call shares it and clears the part it
+ * uses, so calls whose GPU work overlaps (different streams or threads)
+ * race: serialise them.  The call enqueues on `stream` and waits for it to
+ * report device-side errors.  The first call on a device looks the array's
+ * device address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  No counterpart in the reference: there, the CRT and
+ * carry stages (src/crt_gpu.cu, src/carry_prop.cu) need buffers the caller
+ * allocates with cudaMalloc. */
+int bw_garner_carry_noalloc(int path, int num_primes, const void* residues, size_t n,
+                            uint32_t* out, size_t out_words, void* stream);
+
 /* One-shot convenience: plan + context + multiply + teardown, host pointers.
  * (Reference: host_multiply_merge, src/host_multiply.cpp:27-86.) */
 int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b,
