@@ -28,7 +28,8 @@ BW_PTR_HOST = 0
 BW_PTR_DEVICE = 1
 
 BW_PLAN_RADIX8 = 1 << 16
-BW_PLAN_TW_GLOBAL = 1 << 17
+BW_PLAN_TW_SMEM = 1 << 17
+BW_PLAN_THREE_PASS = 1 << 18
 
 _NAMES = {
     BW_EINVAL: "BW_EINVAL", BW_ENOMEM: "BW_ENOMEM", BW_ECUDA: "BW_ECUDA",

@@ -111,7 +111,9 @@ int bw_path_max_log_n(int path, int K) {
     const uint64_t* P = path == BW_PATH_P64 ? kP64 : kP32;
     int m = 64;
     for (int k = 0; k < K; ++k) m = std::min(m, v2(P[k] - 1));
-    const int design = path == BW_PATH_P64 ? 26 : 26;  // two-level 4-step limit
+    // three-pass schedule: C <= 2^12, R, R2 <= 2^11 (larger sizes are bounded
+    // by device memory, checked when the context is allocated)
+    const int design = 34;
     return std::min(m, design);
 }
 
@@ -125,6 +127,8 @@ struct bw_plan {
     int log_n = 0, log_r = 0, log_c = 0, log_cb = 0, lo = 0;
     int tw_smem_r = 0;   // column stage twiddles staged in shared memory
     int rlog_row = 4;    // radix of the row kernel's rounds (2^3 or 2^4)
+    int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)
+    int log_cb2 = 0, lo_out = 0;
     int device = 0;
     bool zt_a = false, zt_b = false;
     void* d_tables = nullptr;
@@ -189,24 +193,36 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     const uint64_t* P = pl->path == BW_PATH_P64 ? kP64 : kP32;
     const uint64_t* Gn = pl->path == BW_PATH_P64 ? kG64 : kG32;
     TableBuilder<Ar> tb;
-    size_t off[kMaxPrimes][8];
+    size_t off[kMaxPrimes][12];
     const size_t n = (size_t)1 << pl->log_n;
+    // row-level twiddle length: R * C (two passes) or R2 * C (three passes)
+    const int log_rr = pl->log_r2 ? pl->log_r2 : pl->log_r;
+    const size_t n_row = (size_t)1 << (log_rr + pl->log_c);
     for (int k = 0; k < pl->K; ++k) {
         const uint64_t p = P[k];
         const uint64_t wn = powmod(Gn[k], (p - 1) >> pl->log_n, p);  // primitive n-th root
-        const uint64_t wni = invmod(wn, p);
-        const uint64_t wr = powmod(wn, (uint64_t)1 << pl->log_c, p);  // R-th root
-        const uint64_t wc = powmod(wn, (uint64_t)1 << pl->log_r, p);  // C-th root
+        const uint64_t wrow = powmod(wn, n / n_row, p);               // n_row-th root
+        const uint64_t wrowi = invmod(wrow, p);
+        const uint64_t wr = powmod(wn, n >> pl->log_r, p);            // R-th root
+        const uint64_t wc = powmod(wn, n >> pl->log_c, p);            // C-th root
         off[k][0] = tb.add_stage_table(p, wr, pl->log_r, bits);
         off[k][1] = tb.add_stage_table(p, invmod(wr, p), pl->log_r, bits);
         off[k][2] = tb.add_stage_table(p, wc, pl->log_c, bits);
         off[k][3] = tb.add_stage_table(p, invmod(wc, p), pl->log_c, bits);
-        const size_t nlo = (size_t)1 << pl->lo, nhi = n >> pl->lo;
+        const size_t nlo = (size_t)1 << pl->lo, nhi = n_row >> pl->lo;
         const uint64_t scale = mulmod(invmod(n % p, p), powmod(2, bits, p), p);
-        off[k][4] = tb.add_power_table(p, wn, nlo, 1, bits);
-        off[k][5] = tb.add_power_table(p, powmod(wn, nlo, p), nhi, 1, bits);
-        off[k][6] = tb.add_power_table(p, wni, nlo, 1, bits);
-        off[k][7] = tb.add_power_table(p, powmod(wni, nlo, p), nhi, scale, bits);
+        off[k][4] = tb.add_power_table(p, wrow, nlo, 1, bits);
+        off[k][5] = tb.add_power_table(p, powmod(wrow, nlo, p), nhi, 1, bits);
+        off[k][6] = tb.add_power_table(p, wrowi, nlo, 1, bits);
+        off[k][7] = tb.add_power_table(p, powmod(wrowi, nlo, p), nhi, scale, bits);
+        if (pl->log_r2) {
+            const uint64_t wm = powmod(wn, n >> pl->log_r2, p);  // R2-th root
+            off[k][8] = tb.add_stage_table(p, wm, pl->log_r2, bits);
+            off[k][9] = tb.add_stage_table(p, invmod(wm, p), pl->log_r2, bits);
+            const size_t olo = (size_t)1 << pl->lo_out, ohi = n >> pl->lo_out;
+            off[k][10] = tb.add_power_table(p, wn, olo, 1, bits);
+            off[k][11] = tb.add_power_table(p, powmod(wn, olo, p), ohi, 1, bits);
+        }
     }
     pl->table_bytes = tb.host.size() * sizeof(Tw<T>);
     BW_CUDA(cudaMalloc(&pl->d_tables, pl->table_bytes));
@@ -222,6 +238,10 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
         pr.THf = base + off[k][5];
         pr.TLi = base + off[k][6];
         pr.THi = base + off[k][7];
+        pr.WMf = pl->log_r2 ? base + off[k][8] : nullptr;
+        pr.WMi = pl->log_r2 ? base + off[k][9] : nullptr;
+        pr.OLf = pl->log_r2 ? base + off[k][10] : nullptr;
+        pr.OHf = pl->log_r2 ? base + off[k][11] : nullptr;
         pr.ar.p = (T)P[k];
         pr.ar.p2 = (T)(2 * P[k]);
         pr.ar.pinv = (T)neg_inv_pow2(P[k], bits);
@@ -247,6 +267,9 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     pd.log_cb = pl->log_cb;
     pd.tw_smem_r = pl->tw_smem_r;
     pd.log_fa = pl->log_c / 2;
+    pd.log_r2 = pl->log_r2;
+    pd.log_cb2 = pl->log_cb2;
+    pd.lo_out = pl->lo_out;
     return BW_OK;
 }
 
@@ -313,25 +336,57 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     pl->log_n = log_n;
     const int w = path == BW_PATH_P64 ? 8 : 4;
     const int max_c = path == BW_PATH_P64 ? 13 : 14;
-    pl->log_c = std::min(max_c, (log_n + 1) / 2);
+    // two passes per transform while the column length fits a CTA (R <= 2^13),
+    // three passes (n = R * R2 * C) beyond, or when asked for
+    const bool three = (flags & BW_PLAN_THREE_PASS) || log_n > 26;
     const int want_c = (int)((flags >> 8) & 0x1f);
-    if (want_c) {
-        if (want_c > max_c || want_c >= log_n || log_n - want_c > 13) {
-            delete pl;
-            return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c, log_n);
+    if (!three) {
+        pl->log_c = std::min(max_c, (log_n + 1) / 2);
+        if (want_c) {
+            if (want_c > max_c || want_c >= log_n || log_n - want_c > 13) {
+                delete pl;
+                return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c,
+                               log_n);
+            }
+            pl->log_c = want_c;
         }
-        pl->log_c = want_c;
+        pl->log_r = log_n - pl->log_c;
+    } else {
+        pl->log_c = std::min(12, log_n - 2);
+        if (want_c) {
+            if (want_c > max_c || want_c > log_n - 2 || log_n - want_c > 22) {
+                delete pl;
+                return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c,
+                               log_n);
+            }
+            pl->log_c = want_c;
+        }
+        const int rem = log_n - pl->log_c;
+        pl->log_r = (rem + 1) / 2;
+        pl->log_r2 = rem - pl->log_r;
+        if (pl->log_r > 11 || pl->log_r2 > 11) {
+            delete pl;
+            return bw_fail(BW_ESIZE, "transform length 2^%d beyond the three-pass schedule",
+                           log_n);
+        }
     }
-    pl->log_r = log_n - pl->log_c;
+    const int log_cols_outer = pl->log_c + pl->log_r2;  // row length of the outer pass
     // column tile: 64 KiB of residues per shared-memory buffer
     int log_cb = 0;
-    while (log_cb < pl->log_c && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536) ++log_cb;
+    while (log_cb < log_cols_outer && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536) ++log_cb;
     pl->log_cb = log_cb;
-    // stage the R-point twiddles in shared memory when they take <= 32 KiB
-    pl->tw_smem_r = ((size_t)2 * w << pl->log_r) <= 32768 ? 1 : 0;
-    if (flags & BW_PLAN_TW_GLOBAL) pl->tw_smem_r = 0;
+    if (pl->log_r2) {
+        int l2 = 0;
+        while (l2 < pl->log_c && ((size_t)w << (pl->log_r2 + l2 + 1)) <= 65536) ++l2;
+        pl->log_cb2 = l2;
+    }
+    // column stage twiddles: read through L1 by default (measured faster than
+    // staging them in shared memory, which costs occupancy); staging on
+    // request when they take <= 32 KiB
+    pl->tw_smem_r = ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
     pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
-    pl->lo = (log_n + 1) / 2;
+    pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
+    pl->lo_out = (log_n + 1) / 2;
     const size_t half = ((size_t)1 << log_n) / 2;
     pl->zt_a = pl->nca <= half;
     pl->zt_b = pl->ncb <= half;
@@ -544,6 +599,8 @@ int set_smem_attrs() {
         set((const void*)k_row<Ar, 128, 3>);
         set((const void*)k_row<Ar, 256, 3>);
         set((const void*)k_row<Ar, 512, 3>);
+        set((const void*)k_mid_col<Ar, false>);
+        set((const void*)k_mid_col<Ar, true>);
     });
     if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
     return BW_OK;
@@ -552,7 +609,7 @@ int set_smem_attrs() {
 template <class Ar, int RLOG>
 void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
                 const typename Ar::T* rb, int sq, size_t smem, cudaStream_t s) {
-    dim3 g(1u << pl->log_r, pl->K);
+    dim3 g(1u << (pl->log_r + pl->log_r2), pl->K);
     // one thread per sub-problem of a round, 64..512 threads
     const int want = std::min(512, std::max(64, 1 << (pl->log_c - RLOG)));
     switch (want) {
@@ -579,7 +636,8 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const size_t tw_bytes = ts ? (size_t)R * sizeof(Tw<T>) : 0;
 
     const size_t smem1 = tw_bytes + (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
-    dim3 g1(C / CB, 1, square ? 1 : 2);
+    const int cols_outer = 1 << (pl->log_c + pl->log_r2);
+    dim3 g1(cols_outer / CB, 1, square ? 1 : 2);
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     if (ts) {
         k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(
@@ -587,6 +645,14 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     } else {
         k_fwd_col<Ar, SPLIT16, 4, false><<<g1, kColThreads, smem1, c->stream>>>(
             pd, a, pl->nca, b, pl->ncb, ra, rb, zt);
+    }
+    // three passes: middle column pass with the outer twiddle
+    const int CB2 = 1 << pl->log_cb2;
+    const size_t smem_mid = (((size_t)1 << pl->log_r2) + CB2) * sizeof(Tw<T>) +
+                            ((size_t)CB2 << pl->log_r2) * sizeof(T);
+    if (pl->log_r2) {
+        dim3 gm(C / CB2, R, pl->K * (square ? 1 : 2));
+        k_mid_col<Ar, false><<<gm, kColThreads, smem_mid, c->stream>>>(pd, ra, rb);
     }
     if (timing) cudaEventRecord(c->ev[2], c->stream);
 
@@ -602,8 +668,12 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     }
     if (timing) cudaEventRecord(c->ev[3], c->stream);
 
+    if (pl->log_r2) {
+        dim3 gm(C / CB2, R, pl->K);
+        k_mid_col<Ar, true><<<gm, kColThreads, smem_mid, c->stream>>>(pd, ra, ra);
+    }
     const size_t smem3 = tw_bytes + (size_t)R * CB * sizeof(T);
-    dim3 g3(C / CB, pl->K);
+    dim3 g3(cols_outer / CB, pl->K);
     if (ts) {
         k_inv_col<Ar, 4, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
     } else {

@@ -52,10 +52,14 @@ struct PrimeDev {
     const Tw<T>* WRi;  // column inverse
     const Tw<T>* WCf;  // row (C-point) forward, C entries
     const Tw<T>* WCi;  // row inverse
-    const Tw<T>* TLf;  // w_n^e for e < 2^lo
-    const Tw<T>* THf;  // w_n^(e 2^lo) for e < n / 2^lo
-    const Tw<T>* TLi;  // w_n^-e
-    const Tw<T>* THi;  // w_n^-(e 2^lo) * n^-1 * 2^bits
+    const Tw<T>* TLf;  // row-level twiddle w_m^e for e < 2^lo (m = R_row * C,
+    const Tw<T>* THf;  //   R_row the last column length): w_m^(e 2^lo)
+    const Tw<T>* TLi;  // w_m^-e
+    const Tw<T>* THi;  // w_m^-(e 2^lo) * n^-1 * 2^bits
+    const Tw<T>* WMf;  // three-pass schedule: middle (R2-point) stage twiddles
+    const Tw<T>* WMi;
+    const Tw<T>* OLf;  // three-pass schedule: outer twiddle w_n^e, e < 2^lo_out
+    const Tw<T>* OHf;  //   w_n^(e 2^lo_out)
     Ar ar;
     T one_q;           // floor(2^bits / p): Shoup companion of 1 (x mod p)
 };
@@ -76,10 +80,12 @@ struct PlanDev {
     PrimeDev<Ar> pr[kMaxPrimes];
     GarnerDev<Ar> gar;
     int K;
-    int log_n, log_r, log_c, lo;  // lo: split of the inter-pass exponent
-    int log_cb;                   // column tile width CB = 2^log_cb
+    int log_n, log_r, log_c, lo;  // lo: split of the row-level twiddle exponent
+    int log_cb;                   // outer column tile width CB = 2^log_cb
     int tw_smem_r;                // stage the R-point twiddles in shared memory
     int log_fa;                   // per-row twiddle split a (F has 2^a entries)
+    // three-pass schedule (n = R * R2 * C): log_r2 > 0, otherwise 0
+    int log_r2, log_cb2, lo_out;
 };
 
 // Carry look-back state of one context.
@@ -283,9 +289,9 @@ k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoe
     const size_t ncoef = op ? ncoef_b : ncoef_a;
     T* res = op ? res_b : res_a;
     const bool zt = ((zt_mask >> op) & 1u) && P.log_r > 0;
-    const int log_r = P.log_r, log_c = P.log_c, log_cb = P.log_cb;
+    const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb;
     const int R = 1 << log_r, CB = 1 << log_cb;
-    const size_t C = (size_t)1 << log_c;
+    const size_t C = (size_t)1 << log_c;  // stride between rows (R2 * C columns)
     const size_t n = (size_t)R * C;
     const int c0 = blockIdx.x << log_cb;
     const int rows_loaded = zt ? R / 2 : R;
@@ -369,9 +375,12 @@ __global__ void __launch_bounds__(NT)
 k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, int square) {
     using T = typename Ar::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int log_r = P.log_r, log_c = P.log_c;
+    const int log_c = P.log_c;
     const int C = 1 << log_c;
-    const size_t n = (size_t)C << log_r;
+    const size_t n = (size_t)1 << P.log_n;  // residues per prime
+    // rows come in groups of R_row = 2^log_rr: the last column pass's length
+    const int log_rr = P.log_r2 ? P.log_r2 : P.log_r;
+    const size_t n_row = (size_t)C << log_rr;  // length of the row-level twiddle
     const int prow = blockIdx.x;
     const int kp = blockIdx.y;
     const PrimeDev<Ar>& pr = P.pr[kp];
@@ -386,8 +395,8 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
     T* bufA = reinterpret_cast<T*>(Gi + ng);
     T* bufB = bufA + C;
 
-    const uint64_t k1 = bitrev((uint32_t)prow, log_r);
-    const uint64_t nmask = n - 1;
+    const uint64_t k1 = bitrev((uint32_t)prow & ((1u << log_rr) - 1), log_rr);
+    const uint64_t nmask = n_row - 1;
     // F[i] = w^(i k1), G[j] = w^(j 2^a k1), Fi[i] = w^(-i k1) (forward tables
     // at exponent n - e), Gi[j] = w^(-j 2^a k1) n^-1 2^bits (inverse tables,
     // whose high table carries the scale)
@@ -395,7 +404,7 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
         if (i < nf) {
             const uint64_t e = ((uint64_t)i * k1) & nmask;
             F[i] = pow_entry(ar, e, P.lo, pr.TLf, pr.THf);
-            Fi[i] = pow_entry(ar, (n - e) & nmask, P.lo, pr.TLf, pr.THf);
+            Fi[i] = pow_entry(ar, (n_row - e) & nmask, P.lo, pr.TLf, pr.THf);
         } else {
             const uint64_t e = (((uint64_t)(i - nf) << la) * k1) & nmask;
             G[i - nf] = pow_entry(ar, e, P.lo, pr.TLf, pr.THf);
@@ -493,6 +502,99 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
     }
 }
 
+// ------------------------------------------------------------------ K1b / K3b
+// Middle column pass of the three-pass schedule (n = R * R2 * C).  Sub-matrix
+// s (blockIdx.y, k1 = bitrev(s) over R) is the contiguous span
+// [s R2 C, (s+1) R2 C) viewed as R2 rows of C; a CTA takes CB2 columns of it
+// for one prime and operand (blockIdx.z = operand * K + prime).  Forward: the
+// outer twiddle w_n^((i2 C + c) k1) on load, then an R2-point forward NTT.
+// Inverse: an R2-point inverse NTT, then w_n^-((i2 C + c) k1) on store.  The
+// twiddle is split as w_n^(i2 C k1) * w_n^(c k1), both factors in per-CTA
+// tables.
+template <class Ar, bool INV>
+__global__ void __launch_bounds__(kColThreads)
+k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
+    using T = typename Ar::T;
+    constexpr int RLOG = 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int log_r2 = P.log_r2, log_c = P.log_c, log_cb = P.log_cb2;
+    const int R2 = 1 << log_r2, CB = 1 << log_cb;
+    const size_t C = (size_t)1 << log_c;
+    const size_t n = (size_t)1 << P.log_n;
+    const int s = blockIdx.y;
+    const int kp = blockIdx.z % P.K;
+    const int op = blockIdx.z / P.K;
+    const PrimeDev<Ar>& pr = P.pr[kp];
+    const Ar ar = pr.ar;
+    T* g = (op ? res_b : res_a) + (size_t)kp * n + ((size_t)s << (log_r2 + log_c));
+    const int c0 = blockIdx.x << log_cb;
+    Tw<T>* Trow = reinterpret_cast<Tw<T>*>(smem_raw);  // R2 entries
+    Tw<T>* Tcol = Trow + R2;                             // CB entries
+    T* buf = reinterpret_cast<T*>(Tcol + CB);
+
+    const uint64_t k1 = bitrev((uint32_t)s, P.log_r);
+    const uint64_t nmask = n - 1;
+    for (int i = threadIdx.x; i < R2 + CB; i += blockDim.x) {
+        uint64_t e = i < R2 ? (((uint64_t)i << log_c) * k1) & nmask
+                            : ((uint64_t)(c0 + i - R2) * k1) & nmask;
+        if (INV) e = (n - e) & nmask;
+        const Tw<T> t = pow_entry(ar, e, P.lo_out, pr.OLf, pr.OHf);
+        if (i < R2) {
+            Trow[i] = t;
+        } else {
+            Tcol[i - R2] = t;
+        }
+    }
+    __syncthreads();
+
+    const int nr = sched_rounds<RLOG>(log_r2);
+    if constexpr (!INV) {
+        for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x) {
+            const int i2 = e >> log_cb, v = e & (CB - 1);
+            const Tw<T> a = Tcol[v], b = Trow[i2];
+            buf[swz<T>(e)] = ar.shoup(ar.shoup(g[((size_t)i2 << log_c) + c0 + v], a.w, a.wq),
+                                      b.w, b.wq);
+        }
+        __syncthreads();
+        for (int r = 0; r < nr; ++r) {
+            const bool last = (r == nr - 1);
+            auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
+            auto st = [&](int v, int idx, T val) {
+                if (last) {
+                    g[((size_t)idx << log_c) + c0 + v] = val;
+                } else {
+                    buf[swz<T>((idx << log_cb) + v)] = val;
+                }
+            };
+            run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
+                                                 sched_s0<RLOG>(log_r2, r), pr.WMf, ar, false,
+                                                 ld, st);
+            __syncthreads();
+        }
+    } else {
+        for (int r = nr - 1; r >= 0; --r) {
+            const bool first = (r == nr - 1), last = (r == 0);
+            auto ld = [&](int v, int idx) -> T {
+                if (first) return g[((size_t)idx << log_c) + c0 + v];
+                return buf[swz<T>((idx << log_cb) + v)];
+            };
+            auto st = [&](int v, int idx, T val) {
+                if (last) {
+                    const Tw<T> a = Tcol[v], b = Trow[idx];
+                    g[((size_t)idx << log_c) + c0 + v] =
+                        ar.shoup(ar.shoup(val, a.w, a.wq), b.w, b.wq);
+                } else {
+                    buf[swz<T>((idx << log_cb) + v)] = val;
+                }
+            };
+            run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
+                                                sched_s0<RLOG>(log_r2, r), pr.WMi, ar, false, ld,
+                                                st);
+            __syncthreads();
+        }
+    }
+}
+
 // ------------------------------------------------------------------ K3
 // Inverse column pass for prime blockIdx.y, column tile blockIdx.x.  Writes
 // fully reduced residues of the cyclic convolution in natural order, in place.
@@ -503,7 +605,7 @@ k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
     using T = typename Ar::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) cst->counter = 0;
-    const int log_r = P.log_r, log_c = P.log_c, log_cb = P.log_cb;
+    const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb;
     const int R = 1 << log_r;
     const size_t C = (size_t)1 << log_c;
     const size_t n = (size_t)R * C;

@@ -74,10 +74,13 @@ extern "C" {
 /* Split the transform into rows x 2^x columns for the 4-step schedule
  * (0 = automatic).  x <= 13 (64-bit path) or 14 (32-bit path). */
 #define BW_PLAN_LOG_COLS(x) (((unsigned)(x) & 0x1fu) << 8)
-/* Tuning switches: radix-8 instead of radix-16 rounds in the row pass; keep
- * the column stage twiddles in global memory instead of shared memory. */
-#define BW_PLAN_RADIX8     (1u << 16)
-#define BW_PLAN_TW_GLOBAL  (1u << 17)
+/* Tuning switches: radix-8 instead of radix-16 rounds in the row pass;
+ * stage the column stage twiddles in shared memory (when <= 32 KiB) instead
+ * of reading them through L1; use the three-pass schedule (n = R * R2 * C)
+ * even where two passes fit (it is used anyway beyond n = 2^26). */
+#define BW_PLAN_RADIX8      (1u << 16)
+#define BW_PLAN_TW_SMEM     (1u << 17)
+#define BW_PLAN_THREE_PASS  (1u << 18)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):

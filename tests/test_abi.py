@@ -35,14 +35,15 @@ def test_abi_version():
 def test_limits():
     l64 = bw.limits(bw.BW_PATH_P64)
     l32 = bw.limits(bw.BW_PATH_P32)
-    assert l64["max_log_n"] >= 24 and l64["num_primes"] == 2
+    assert l64["max_log_n"] == 32 and l64["num_primes"] == 2
     assert l32["max_log_n"] == 24
     assert l32["max_square_words"] == (1 << 23) // 2
     assert bw.limits(bw.BW_PATH_P64, 3)["num_primes"] == 3
 
 
 @pytest.mark.parametrize("la,lb,path,ok", [
-    (1, 1, 64, True), (1 << 23, 1 << 23, 64, True), (1 << 15, 1 << 15, 32, True),
+    (1, 1, 64, True), (1 << 23, 1 << 23, 64, True), (1 << 28, 1 << 28, 64, True),
+    (1 << 31, 1 << 31, 64, True), (1 << 32, 1 << 32, 64, False), (1 << 15, 1 << 15, 32, True),
     (1 << 23, 1 << 23, 32, False),   # 2^24 16-bit coefficients each -> n = 2^25
     (0, 5, 64, False), (5, 0, 32, False),
 ])
@@ -61,7 +62,7 @@ def test_bad_arguments_are_reported_not_fatal():
     assert bw.lib.bw_plan_create(ctypes.byref(h), 64, 0, 4, 0, 0) == _lib.BW_ESIZE
     assert bw.lib.bw_plan_create(None, 64, 4, 4, 0, 0) == _lib.BW_EINVAL
     with pytest.raises(bw.BwError) as e:
-        bw.Plan(1 << 26, 1 << 26, bw.BW_PATH_P64)
+        bw.Plan(1 << 32, 1 << 32, bw.BW_PATH_P64)   # n = 2^33 > v2(p - 1) = 32
     assert e.value.code == _lib.BW_ESIZE
 
 

@@ -261,3 +261,53 @@ def test_config2_three_primes_properties():
     for m in (2 ** 64, 2 ** 61 - 1, 1000000007, 998244353, (1 << 31) - 1):
         assert C % m == (A % m) * (B % m) % m
     assert C.bit_length() <= 64 * (1 << 23)
+
+
+@pytest.mark.parametrize("path,K", PATHS)
+def test_three_pass_schedule_vs_oracle(path, K):
+    # the n = R * R2 * C schedule (used beyond n = 2^26), forced at small sizes
+    flags = bw._lib.BW_PLAN_THREE_PASS
+    rng = np.random.default_rng(200 + path + K)
+    for la, lb in [(1, 1), (8, 8), (9, 8), (100, 77), (1000, 1000), (4096, 3000), (5000, 1)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        with bw.Plan(la, lb, path, K, flags=flags) as p, bw.Context(p) as c:
+            assert p.info["log_rows"] >= 1
+            got = c.multiply(a, b)
+            sq = c.square(a) if la == lb else None
+        assert (got == oracle.multiply(a, b, path, K)).all(), (la, lb)
+        if sq is not None:
+            assert (sq == oracle.multiply(a, a, path, K)).all(), la
+
+
+def test_three_pass_schedule_vs_gmp_medium():
+    flags = bw._lib.BW_PLAN_THREE_PASS
+    rng = np.random.default_rng(17)
+    for la, lb, path, K in [(1 << 16, 1 << 16, 64, 2), ((1 << 19) + 5, (1 << 18) - 3, 64, 3),
+                            (1 << 18, 1 << 18, 32, 2), (1 << 20, 1 << 20, 64, 2)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        with bw.Plan(la, lb, path, K, flags=flags) as p, bw.Context(p) as c:
+            got = c.multiply(a, b)
+        assert (got == gmp_ref.mul(a, b)).all(), (la, lb, path, K)
+
+
+def test_config4_plain_huge():
+    # 2^33-bit operands (2^28 words, 1 GiB each),
+    # 32-bit coefficients, n = 2^29, three 62-bit primes, three-pass
+    # schedule.  Checked by residues mod 2^64 and mod three random 61-bit
+    # primes, and bit-exact against GMP mpz_mul on the host.
+    a = mt64.random_words_top_fast(1 << 28, 4321)
+    b = mt64.random_words_top_fast(1 << 28, 8765)
+    with bw.Plan(a.size, b.size, 64, 3) as p, bw.Context(p) as c:
+        assert p.info["log_n"] == 29 and p.info["num_primes"] == 3
+        got, t = c.multiply(a, b, timing=True)
+    A, B, C = as_int(a), as_int(b), as_int(got)
+    rng = np.random.default_rng(61)
+    mods = [1 << 64]
+    while len(mods) < 4:
+        m = int(rng.integers(1 << 60, 1 << 61)) | 1
+        if pow(3, m - 1, m) == 1:  # probable prime
+            mods.append(m)
+    for m in mods:
+        assert C % m == (A % m) * (B % m) % m, m
+    del A, B, C
+    assert (got == gmp_ref.mul(a, b)).all()
