@@ -48,6 +48,16 @@ CONFIGS = {
              "plain 2^26-bit x 2^26-bit, 32-bit coefficients, n=2^22, 2 x 62-bit primes"),
 }
 
+# batched configurations: (products, seed, K, description)
+BATCH_CONFIGS = {
+    "3": (4096, 3, 2,
+          "batched uneven sizes: 4096 products, operands 2^12..2^20 bits log-uniform, second "
+          "operand 1/8x..1x, half on the 32-bit path (16-bit coefficients), half on the "
+          "64-bit path (32-bit coefficients), 2 primes each"),
+    # the same mix at 1/8 of the products, for ncu captures
+    "3prof": (512, 3, 2, "batched uneven sizes, 512 products of the same mix"),
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -55,9 +65,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--autotune", action="store_true",
+                    help="batched configurations: tune each bucket's kernel form first")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batched configurations: skip the plain per-product loop")
     ap.add_argument("--log-cols", type=int, default=0,
                     help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")
     ap.add_argument("--plan-flags", type=lambda s: int(s, 0), default=0,
@@ -224,8 +238,263 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def batch_items(cfg, rank):
+    from birdwing_b200 import workloads
+    count, seed, K, _ = BATCH_CONFIGS[cfg]
+    return workloads.batch_mix(count, seed=seed + 100 * rank), K
+
+
+def batch_model_bytes(items, K, small_max=None):
+    """Algorithmic HBM bytes of a batch: per product the plain path's model
+    (12*K*n*w + in + out) for 4-step products, and in + out + 2*K*n*w (one
+    residue write and read) for products run one CTA each."""
+    small_max = small_max or {64: 13, 32: 14}
+    total = 0
+    for p, a, b in items:
+        cpw = 2 if p == 32 else 1
+        w = 8 if p == 64 else 4
+        log_n = max(4, ((len(a) + len(b)) * cpw - 2).bit_length())
+        knw = K * (1 << log_n) * w
+        io = 4 * (len(a) + len(b)) * 2
+        total += io + (2 * knw if log_n <= small_max[p] else 12 * knw)
+    return total
+
+
+def cpu_baseline_items(items, K, budget_s=20.0):
+    """The oracle on all host threads over the batch's products in order until
+    the budget is spent; GMP mpz_mul (one thread) over all of them."""
+    from oracle import gmp_ref, oracle
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    n_done, t0 = 0, time.perf_counter()
+    for p, a, b in items:
+        oracle.multiply(a, b, p, K)
+        n_done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    g = sum(gmp_ref.time_mul(a, b, 1) for _, a, b in items)
+    return {"value": n_done / dt, "unit": "products/s", "cores": cores, "kind": "port",
+            "sample": f"first {n_done} of {len(items)} products of the mix, oracle/bw_oracle.c "
+                      f"on {cores} threads, {dt:.1f} s",
+            "gmp": {"value": len(items) / g, "unit": "products/s", "cores": 1,
+                    "impl": f"GMP {gmp_ref.version} mpz_mul, single thread, all products"}}
+
+
+def bench_batch(args):
+    """Batched configuration: the whole mix is one step (one graph launch)."""
+    import torch
+    import torch.distributed as dist
+
+    import birdwing_b200 as bw
+    from birdwing_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    items, K = batch_items(args.config, rank)
+    count, _, _, desc = BATCH_CONFIGS[args.config]
+    stream = torch.cuda.Stream()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    # operands in pinned host memory (the batch copies them in and out)
+    pinned = []
+    for p, a, b in items:
+        ha = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        hb = torch.from_numpy(b.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        pinned.append((p, ha, hb))
+    bt = bw.Batch(num_primes=K, stream=stream.cuda_stream)
+    outs = [bt.add(a, b, path=p) for p, a, b in pinned]
+    if args.autotune:
+        bt.autotune(reps=3)
+    bt.run()                                   # layout, graph, upload, compute, download
+    info = bt.info()
+    if rank == 0:
+        from oracle import gmp_ref
+        ok = all(bool((o == gmp_ref.mul(a, b)).all()) for o, (_, a, b) in zip(outs, items))
+    else:
+        ok = True
+    for _ in range(max(3, args.warmup)):
+        bt.run(L.BW_BATCH_COMPUTE)
+
+    sampler = ClockSampler(local)
+    per_step = []
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i)                     # evict L2 between steps
+        t = bt.run(L.BW_BATCH_COMPUTE, timing=True)
+        per_step.append(t["mul_ms"])
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    total_ms = max_over_ranks(sum(per_step))
+
+    # end to end through the public API: host operands in, host results out
+    barrier()
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        bt.run()
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    e2e_total = max_over_ranks(sum(e2e_ms))
+
+    # the plain path looped product by product on the same GPU: one plan and
+    # context per size (built before timing), all on one stream
+    plain = None
+    if not args.no_plain:
+        plans, ctxs, bufs = [], [], []
+        for p, a, b in items:
+            pl = bw.Plan(len(a), len(b), p, K)
+            plans.append(pl)
+            ctxs.append(bw.Context(pl, stream=stream.cuda_stream))
+            da = torch.from_numpy(a.view(np.int32)).cuda()
+            db = torch.from_numpy(b.view(np.int32)).cuda()
+            dc = torch.empty(len(a) + len(b), dtype=torch.int32, device="cuda")
+            bufs.append((da, db, dc))
+
+        def loop():
+            for c, (da, db, dc) in zip(ctxs, bufs):
+                c.multiply_device(da.data_ptr(), da.numel(), db.data_ptr(), db.numel(),
+                                  dc.data_ptr(), dc.numel())
+
+        loop()
+        ctxs[0].sync()
+        if rank == 0:
+            from oracle import gmp_ref
+            for j in range(0, len(items), 97):
+                _, a, b = items[j]
+                assert (bufs[j][2].cpu().numpy().view(np.uint32) == gmp_ref.mul(a, b)).all()
+        reps = max(1, min(args.steps, 5))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            flush.fill_(0)
+            e0.record(stream)
+        for _ in range(reps):
+            loop()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        for c in ctxs:
+            c.sync()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1) / reps)
+        plain = {"value": world * count / (plain_ms * 1e-3), "unit": "products/s",
+                 "ms_per_step": plain_ms, "gpu_launches_per_step": 4 * count,
+                 "how": "bw_multiply (device pointers) per product, one plan+context per "
+                        "product size built beforehand, one stream"}
+        for c in ctxs:
+            c.close()
+        for pl in plans:
+            pl.close()
+
+    if rank == 0:
+        ms = total_ms / args.steps
+        peak, peak_kind = load_peaks()
+        mb = batch_model_bytes(items, K)
+        achieved = mb / (ms * 1e-3) / 1e9
+        launches = info["small_buckets"] + 4 * (info["buckets"] - info["small_buckets"])
+        h2d = sum(4 * (len(a) + len(b)) for _, a, b in items)
+        d2h = sum(4 * (len(a) + len(b)) for _, a, b in items) + 4
+        line = {
+            "metric": "products/s", "value": world * count * args.steps / (total_ms * 1e-3),
+            "unit": "products/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64/u32", "data": "synthetic",
+            "config": {"workload": f"config {args.config}: {desc}", "products": count,
+                       "num_primes": K, "buckets": info["buckets"],
+                       "small_buckets": info["small_buckets"],
+                       "graph_nodes": info["graph_nodes"],
+                       "device_bytes": info["device_bytes"], "autotuned": bool(args.autotune),
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "correct_vs_gmp": ok,
+            "roofline": {"bound": "hbm", "kernel": "batch graph (all buckets, one launch)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": load_traffic(args.config, "batch_graph"),
+                         "algorithmic_bytes": mb},
+            "plain_loop": plain,
+            "batched_over_plain": (world * count * args.steps / (total_ms * 1e-3)) /
+                                  plain["value"] if plain else None,
+            "e2e": {"value": world * count * args.e2e_steps / (e2e_total * 1e-3),
+                    "unit": "products/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+            "tune_table": bw.tune_table() if args.autotune else None,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_items(items, K)
+        print(json.dumps(line))
+    bt.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference_batch(args):
+    """--impl reference on a batched configuration: the oracle over the mix's
+    products in order (a bounded sample), on all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    items, K = batch_items(args.config, 0)
+    count, _, _, desc = BATCH_CONFIGS[args.config]
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    for p, a, b in items[: min(args.warmup, 3)]:
+        oracle.multiply(a, b, p, K)
+    budget = 150.0
+    n_done, t0 = 0, time.perf_counter()
+    for p, a, b in items:
+        oracle.multiply(a, b, p, K)
+        n_done += 1
+        if time.perf_counter() - t0 >= budget:
+            break
+    dt = time.perf_counter() - t0
+    v = n_done / dt
+    line = {
+        "impl": "reference", "metric": "products/s", "value": v, "unit": "products/s",
+        "n_gpus": args.gpus, "steps": 1, "warmup": min(args.warmup, 3),
+        "ms_per_step": 1000 * dt, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64/u32", "data": "synthetic",
+        "config": {"workload": f"config {args.config}: {desc}", "products": count,
+                   "num_primes": K},
+        "cpu_baseline": {"value": v, "unit": "products/s", "cores": cores, "kind": "port",
+                         "sample": f"first {n_done} of {count} products, oracle/bw_oracle.c "
+                                   f"on {cores} threads, {dt:.1f} s"},
+        "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.config in BATCH_CONFIGS:
+        if args.impl == "reference":
+            run_reference_batch(args)
+        else:
+            bench_batch(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

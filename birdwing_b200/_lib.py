@@ -31,6 +31,11 @@ BW_PLAN_RADIX8 = 1 << 16
 BW_PLAN_TW_SMEM = 1 << 17
 BW_PLAN_THREE_PASS = 1 << 18
 
+BW_BATCH_THREE_PRIMES = 1
+BW_BATCH_UPLOAD = 1
+BW_BATCH_COMPUTE = 2
+BW_BATCH_DOWNLOAD = 4
+
 _NAMES = {
     BW_EINVAL: "BW_EINVAL", BW_ENOMEM: "BW_ENOMEM", BW_ECUDA: "BW_ECUDA",
     BW_ETIMEOUT: "BW_ETIMEOUT", BW_EREJECT: "BW_EREJECT", BW_ESIZE: "BW_ESIZE",
@@ -69,6 +74,34 @@ class bw_limits_info(ctypes.Structure):
                 ("max_log_n", ctypes.c_int), ("max_square_words", ctypes.c_size_t)]
 
 
+class bw_batch_info(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_size_t) for n in
+                ("products", "buckets", "small_buckets", "graph_nodes", "device_bytes")]
+
+
+class bw_server_config(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("pinned_bytes", ctypes.c_size_t),
+                ("lanes", ctypes.c_int), ("max_groups_in_flight", ctypes.c_int),
+                ("num_primes", ctypes.c_int), ("path", ctypes.c_int)]
+
+
+class bw_request_info(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("status", ctypes.c_int),
+                ("submit_us", ctypes.c_double), ("admit_us", ctypes.c_double),
+                ("launch_us", ctypes.c_double), ("done_us", ctypes.c_double),
+                ("group_size", ctypes.c_size_t), ("device_bytes", ctypes.c_size_t),
+                ("la", ctypes.c_size_t), ("lb", ctypes.c_size_t)]
+
+
+class bw_server_stats(ctypes.Structure):
+    _fields_ = ([(n, ctypes.c_uint64) for n in ("submitted", "completed", "rejected", "failed",
+                                                  "groups", "kernel_launches")] +
+                [(n, ctypes.c_size_t) for n in ("max_group_size", "bytes_in_flight",
+                                                 "peak_bytes_in_flight", "resident_plan_bytes",
+                                                 "queue_depth", "groups_in_flight",
+                                                 "budget_bytes")])
+
+
 # symbol -> (restype, argtypes)
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
@@ -94,6 +127,25 @@ SIGNATURES = {
     "bw_ctx_inject_wait_fault": (_I, [_P, _I]),
     "bw_multiply_host_once": (_I, [_P, _SZ, _P, _SZ, _P, _SZ, _I,
                                    ctypes.POINTER(ctypes.c_float)]),
+    "bw_batch_create": (_I, [ctypes.POINTER(_P), _P, _U]),
+    "bw_batch_destroy": (_I, [_P]),
+    "bw_batch_clear": (_I, [_P]),
+    "bw_batch_add": (_I, [_P, _I, _P, _SZ, _P, _SZ, _P, _SZ]),
+    "bw_batch_run": (_I, [_P, _U, ctypes.POINTER(bw_timing)]),
+    "bw_batch_get_info": (_I, [_P, ctypes.POINTER(bw_batch_info)]),
+    "bw_batch_autotune": (_I, [_P, _I]),
+    "bw_tune_table_export": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "bw_tune_table_set": (_I, [_I, _I, _I, _I, _I]),
+    "bw_server_create": (_I, [ctypes.POINTER(_P), ctypes.POINTER(bw_server_config)]),
+    "bw_server_destroy": (_I, [_P]),
+    "bw_server_prewarm": (_I, [_P, _I, _I]),
+    "bw_server_submit": (_I, [_P, _I, _P, _SZ, _P, _SZ, _P, _SZ,
+                              ctypes.POINTER(ctypes.c_uint64)]),
+    "bw_server_wait": (_I, [_P, ctypes.c_uint64, _I, ctypes.POINTER(bw_request_info)]),
+    "bw_server_harvest": (_I, [_P, ctypes.POINTER(bw_request_info), _SZ,
+                               ctypes.POINTER(_SZ)]),
+    "bw_server_drain": (_I, [_P, _I]),
+    "bw_server_get_stats": (_I, [_P, ctypes.POINTER(bw_server_stats)]),
 }
 
 

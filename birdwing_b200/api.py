@@ -22,7 +22,8 @@ from ._lib import BwError, check, lib
 
 __all__ = [
     "Plan", "Context", "host_multiply_merge", "host_multiply_merge_native", "multiply",
-    "square", "limits", "size_supported", "int_to_limbs", "limbs_to_int", "BwError",
+    "square", "limits", "size_supported", "int_to_limbs", "limbs_to_int", "BwError", "Batch",
+    "tune_table", "set_tune_entry", "load_tune_table",
 ]
 
 
@@ -225,3 +226,89 @@ def host_multiply_merge_native(A, B):
     B = np.ascontiguousarray(B, dtype=np.uint64)
     out, ms = host_multiply_merge(A.view(np.uint32), B.view(np.uint32))
     return out.view(np.uint64), ms
+
+
+class Batch:
+    """Many independent products of uneven sizes run together (bw_batch_*).
+
+    ``add`` keeps references to the host arrays: every ``run`` re-reads the
+    operands and rewrites the outputs, so a caller can refill the same arrays
+    and run again (the captured graph is replayed while the list of products
+    is unchanged).  The reference has no batched form; its unit is one
+    host_multiply_merge call per product.
+    """
+
+    def __init__(self, num_primes=2, stream=None):
+        h = ctypes.c_void_p()
+        flags = L.BW_BATCH_THREE_PRIMES if num_primes == 3 else 0
+        check(lib.bw_batch_create(ctypes.byref(h), ctypes.c_void_p(stream or 0), flags))
+        self._h = h
+        self._keep = []
+        self.outputs = []
+
+    def add(self, a, b, out=None, path=L.BW_PATH_AUTO):
+        """Append a * b; returns the output array (len(a) + len(b) words)."""
+        a = _as_u32(a)
+        b = a if b is a else _as_u32(b)
+        if out is None:
+            out = np.zeros(a.size + b.size, dtype=np.uint32)
+        check(lib.bw_batch_add(self._h, path, _ptr(a), a.size, _ptr(b), b.size, _ptr(out),
+                               out.size))
+        self._keep.append((a, b, out))
+        self.outputs.append(out)
+        return out
+
+    def clear(self):
+        check(lib.bw_batch_clear(self._h))
+        self._keep = []
+        self.outputs = []
+
+    def run(self, what=0, timing=False):
+        t = L.bw_timing()
+        check(lib.bw_batch_run(self._h, what, ctypes.byref(t) if timing else None))
+        return t.as_dict() if timing else None
+
+    def info(self):
+        i = L.bw_batch_info()
+        check(lib.bw_batch_get_info(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in L.bw_batch_info._fields_}
+
+    def autotune(self, reps=3):
+        check(lib.bw_batch_autotune(self._h, reps))
+
+    def close(self):
+        if self._h:
+            lib.bw_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def tune_table():
+    """The process-wide batch tune table (list of dicts)."""
+    import json
+    need = ctypes.c_size_t()
+    check(lib.bw_tune_table_export(None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(need.value)
+    check(lib.bw_tune_table_export(buf, need.value, ctypes.byref(need)))
+    return json.loads(buf.value.decode())
+
+
+def set_tune_entry(path, num_primes, log_n, small, log_cols=0):
+    check(lib.bw_tune_table_set(path, num_primes, log_n, 1 if small else 0, log_cols))
+
+
+def load_tune_table(entries):
+    """Install entries as produced by tune_table() (e.g. read back from JSON)."""
+    for e in entries:
+        set_tune_entry(e["path"], e["num_primes"], e["log_n"], e["small"], e["log_cols"])

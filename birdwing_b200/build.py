@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbirdwing.so")
-SOURCES = ["bw_core.cu", "bw_noalloc.cu"]
-HEADERS = ["bw_arith.cuh", "bw_kernels.cuh", "bw_host.h"]
+SOURCES = ["bw_core.cu", "bw_noalloc.cu", "bw_batch.cu", "bw_server.cu"]
+HEADERS = ["bw_arith.cuh", "bw_kernels.cuh", "bw_host.h", "bw_internal.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

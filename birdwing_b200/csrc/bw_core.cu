@@ -21,6 +21,7 @@
 
 #include "../../include/birdwing.h"
 #include "bw_host.h"
+#include "bw_internal.h"
 #include "bw_kernels.cuh"
 
 using namespace bw;
@@ -121,23 +122,6 @@ const uint64_t* bw_path_primes(int path) { return path == BW_PATH_P64 ? kP64 : k
 
 // ------------------------------------------------------------------ plan
 
-struct bw_plan {
-    int path = 0, K = 0;
-    size_t la = 0, lb = 0, nca = 0, ncb = 0;
-    int log_n = 0, log_r = 0, log_c = 0, log_cb = 0, lo = 0;
-    int tw_smem_r = 0;   // column stage twiddles staged in shared memory
-    int rlog_row = 4;    // radix of the row kernel's rounds (2^3 or 2^4)
-    int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)
-    int log_cb2 = 0, lo_out = 0;
-    int device = 0;
-    bool zt_a = false, zt_b = false;
-    void* d_tables = nullptr;
-    size_t table_bytes = 0;
-    PlanDev<Ar32> pd32{};
-    PlanDev<Ar64> pd64{};
-    uint64_t primes[3] = {0, 0, 0};
-};
-
 namespace {
 
 template <class Ar>
@@ -198,8 +182,17 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     // row-level twiddle length: R * C (two passes) or R2 * C (three passes)
     const int log_rr = pl->log_r2 ? pl->log_r2 : pl->log_r;
     const size_t n_row = (size_t)1 << (log_rr + pl->log_c);
+    uint64_t scale_k[kMaxPrimes] = {0, 0, 0};
     for (int k = 0; k < pl->K; ++k) {
         const uint64_t p = P[k];
+        scale_k[k] = mulmod(invmod(n % p, p), powmod(2, bits, p), p);
+        if (pl->small) {
+            // single pass: n-point stage tables only
+            const uint64_t wn = powmod(Gn[k], (p - 1) >> pl->log_n, p);
+            off[k][2] = tb.add_stage_table(p, wn, pl->log_n, bits);
+            off[k][3] = tb.add_stage_table(p, invmod(wn, p), pl->log_n, bits);
+            continue;
+        }
         const uint64_t wn = powmod(Gn[k], (p - 1) >> pl->log_n, p);  // primitive n-th root
         const uint64_t wrow = powmod(wn, n / n_row, p);               // n_row-th root
         const uint64_t wrowi = invmod(wrow, p);
@@ -230,6 +223,17 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     const Tw<T>* base = reinterpret_cast<const Tw<T>*>(pl->d_tables);
     for (int k = 0; k < pl->K; ++k) {
         auto& pr = pd.pr[k];
+        pr.scale = Tw<T>{(T)scale_k[k], (T)shoup_pre(scale_k[k], P[k], bits)};
+        if (pl->small) {
+            pr.WCf = base + off[k][2];
+            pr.WCi = base + off[k][3];
+            pr.ar.p = (T)P[k];
+            pr.ar.p2 = (T)(2 * P[k]);
+            pr.ar.pinv = (T)neg_inv_pow2(P[k], bits);
+            set_c(pr.ar, P[k]);
+            pr.one_q = (T)shoup_pre(1, P[k], bits);
+            continue;
+        }
         pr.WRf = base + off[k][0];
         pr.WRi = base + off[k][1];
         pr.WCf = base + off[k][2];
@@ -315,6 +319,76 @@ static int choose_path(size_t la, size_t lb) {
     return BW_PATH_P64;
 }
 
+int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int mode) {
+    pl->path = path;
+    pl->K = K;
+    pl->log_n = log_n;
+    const int w = path == BW_PATH_P64 ? 8 : 4;
+    const int max_c = path == BW_PATH_P64 ? 13 : 14;
+    if (mode == 1) {
+        pl->small = 1;
+        pl->log_c = log_n;
+        pl->log_r = 0;
+    } else {
+        // two passes per transform while the column length fits a CTA
+        // (R <= 2^13), three passes (n = R * R2 * C) beyond, or when asked for
+        const bool three = (flags & BW_PLAN_THREE_PASS) || log_n > 26;
+        const int want_c = (int)((flags >> 8) & 0x1f);
+        if (!three) {
+            pl->log_c = std::min(max_c, (log_n + 1) / 2);
+            if (want_c) {
+                if (want_c > max_c || want_c >= log_n || log_n - want_c > 13)
+                    return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d",
+                                   want_c, log_n);
+                pl->log_c = want_c;
+            }
+            pl->log_r = log_n - pl->log_c;
+        } else {
+            pl->log_c = std::min(12, log_n - 2);
+            if (want_c) {
+                if (want_c > max_c || want_c > log_n - 2 || log_n - want_c > 22)
+                    return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d",
+                                   want_c, log_n);
+                pl->log_c = want_c;
+            }
+            const int rem = log_n - pl->log_c;
+            pl->log_r = (rem + 1) / 2;
+            pl->log_r2 = rem - pl->log_r;
+            if (pl->log_r > 11 || pl->log_r2 > 11)
+                return bw_fail(BW_ESIZE, "transform length 2^%d beyond the three-pass schedule",
+                               log_n);
+        }
+        const int log_cols_outer = pl->log_c + pl->log_r2;  // row length of the outer pass
+        // column tile: 64 KiB of residues per shared-memory buffer
+        int log_cb = 0;
+        while (log_cb < log_cols_outer && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536)
+            ++log_cb;
+        pl->log_cb = log_cb;
+        if (pl->log_r2) {
+            int l2 = 0;
+            while (l2 < pl->log_c && ((size_t)w << (pl->log_r2 + l2 + 1)) <= 65536) ++l2;
+            pl->log_cb2 = l2;
+        }
+        // column stage twiddles: read through L1 by default (measured faster
+        // than staging them in shared memory, which costs occupancy); staged on
+        // request when they take <= 32 KiB
+        pl->tw_smem_r =
+            ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
+        pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
+        pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
+        pl->lo_out = (log_n + 1) / 2;
+    }
+    for (int k = 0; k < K; ++k) pl->primes[k] = bw_path_primes(path)[k];
+    cudaGetDevice(&pl->device);
+    const int rc =
+        path == BW_PATH_P64 ? build_tables<Ar64>(pl, pl->pd64) : build_tables<Ar32>(pl, pl->pd32);
+    if (rc && pl->d_tables) {
+        cudaFree(pl->d_tables);
+        pl->d_tables = nullptr;
+    }
+    return rc;
+}
+
 extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int num_primes,
                               unsigned flags) {
     bw_clear_error();
@@ -326,75 +400,16 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     int rc = bw_check_size(path, K, la, lb, &log_n);
     if (rc) return rc;
     bw_plan* pl = new bw_plan();
-    pl->path = path;
-    pl->K = K;
     pl->la = la;
     pl->lb = lb;
     const int cpw = path == BW_PATH_P32 ? 2 : 1;
     pl->nca = la * cpw;
     pl->ncb = lb * cpw;
-    pl->log_n = log_n;
-    const int w = path == BW_PATH_P64 ? 8 : 4;
-    const int max_c = path == BW_PATH_P64 ? 13 : 14;
-    // two passes per transform while the column length fits a CTA (R <= 2^13),
-    // three passes (n = R * R2 * C) beyond, or when asked for
-    const bool three = (flags & BW_PLAN_THREE_PASS) || log_n > 26;
-    const int want_c = (int)((flags >> 8) & 0x1f);
-    if (!three) {
-        pl->log_c = std::min(max_c, (log_n + 1) / 2);
-        if (want_c) {
-            if (want_c > max_c || want_c >= log_n || log_n - want_c > 13) {
-                delete pl;
-                return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c,
-                               log_n);
-            }
-            pl->log_c = want_c;
-        }
-        pl->log_r = log_n - pl->log_c;
-    } else {
-        pl->log_c = std::min(12, log_n - 2);
-        if (want_c) {
-            if (want_c > max_c || want_c > log_n - 2 || log_n - want_c > 22) {
-                delete pl;
-                return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d", want_c,
-                               log_n);
-            }
-            pl->log_c = want_c;
-        }
-        const int rem = log_n - pl->log_c;
-        pl->log_r = (rem + 1) / 2;
-        pl->log_r2 = rem - pl->log_r;
-        if (pl->log_r > 11 || pl->log_r2 > 11) {
-            delete pl;
-            return bw_fail(BW_ESIZE, "transform length 2^%d beyond the three-pass schedule",
-                           log_n);
-        }
-    }
-    const int log_cols_outer = pl->log_c + pl->log_r2;  // row length of the outer pass
-    // column tile: 64 KiB of residues per shared-memory buffer
-    int log_cb = 0;
-    while (log_cb < log_cols_outer && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536) ++log_cb;
-    pl->log_cb = log_cb;
-    if (pl->log_r2) {
-        int l2 = 0;
-        while (l2 < pl->log_c && ((size_t)w << (pl->log_r2 + l2 + 1)) <= 65536) ++l2;
-        pl->log_cb2 = l2;
-    }
-    // column stage twiddles: read through L1 by default (measured faster than
-    // staging them in shared memory, which costs occupancy); staging on
-    // request when they take <= 32 KiB
-    pl->tw_smem_r = ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
-    pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
-    pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
-    pl->lo_out = (log_n + 1) / 2;
     const size_t half = ((size_t)1 << log_n) / 2;
     pl->zt_a = pl->nca <= half;
     pl->zt_b = pl->ncb <= half;
-    for (int k = 0; k < K; ++k) pl->primes[k] = bw_path_primes(path)[k];
-    cudaGetDevice(&pl->device);
-    rc = path == BW_PATH_P64 ? build_tables<Ar64>(pl, pl->pd64) : build_tables<Ar32>(pl, pl->pd32);
+    rc = bw_plan_setup(pl, path, K, log_n, flags, 0);
     if (rc) {
-        if (pl->d_tables) cudaFree(pl->d_tables);
         delete pl;
         return rc;
     }
@@ -413,7 +428,7 @@ static size_t ctx_bytes(const bw_plan* pl) {
     const size_t n = (size_t)1 << pl->log_n;
     const int w = pl->path == BW_PATH_P64 ? 8 : 4;
     const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
-    const size_t nl = n / cpw;
+    const size_t nl = std::max(n / cpw, pl->la + pl->lb);
     const size_t ntiles = (nl + kCarryTileWords - 1) / kCarryTileWords;
     return 2 * (size_t)pl->K * n * w + (pl->la + pl->lb) * 4 * 2 + 64 + ntiles * 20;
 }
@@ -488,7 +503,10 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
         (e = cudaMalloc(&c->d_out, ((pl->la + pl->lb + 3) & ~(size_t)3) * 4)) != cudaSuccess)
         return fail(bw_fail(BW_ENOMEM, "context allocation (%zu bytes of residues x2): %s",
                             res_bytes, cudaGetErrorString(e)));
-    c->ntiles = (n / cpw + kCarryTileWords - 1) / kCarryTileWords;
+    // carry tiles cover the n / cpw coefficient words and the product's words
+    // (la + lb can be n / cpw + 1 when la + lb - 1 is a power of two)
+    const size_t words = std::max(n / cpw, pl->la + pl->lb);
+    c->ntiles = (words + kCarryTileWords - 1) / kCarryTileWords;
     c->state_bytes = 32 + c->ntiles * 16 + c->ntiles * 4;
     if ((e = cudaMalloc(&c->d_state, c->state_bytes)) != cudaSuccess)
         return fail(bw_fail(BW_ENOMEM, "carry state: %s", cudaGetErrorString(e)));
@@ -605,6 +623,16 @@ int set_smem_attrs() {
     if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
     return BW_OK;
 }
+
+}  // namespace
+
+int bw_set_kernel_attrs() {
+    int rc = set_smem_attrs<Ar64, false>();
+    if (!rc) rc = set_smem_attrs<Ar32, true>();
+    return rc;
+}
+
+namespace {
 
 template <class Ar, int RLOG>
 void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,

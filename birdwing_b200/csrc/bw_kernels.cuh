@@ -62,6 +62,7 @@ struct PrimeDev {
     const Tw<T>* OHf;  //   w_n^(e 2^lo_out)
     Ar ar;
     T one_q;           // floor(2^bits / p): Shoup companion of 1 (x mod p)
+    Tw<T> scale;       // n^-1 * 2^bits (single-pass transforms of small products)
 };
 
 // Garner constants (reference: CRTGarnerParams, include/crt_gpu.h:11-17,
@@ -92,6 +93,22 @@ struct PlanDev {
 struct CarryState {
     uint32_t counter;   // dynamic tile ticket (reset by K3 before every K4)
     uint32_t pad[3];
+};
+
+// One product of a batch (device memory).  Residues of product i live at
+// element offset res_off of the bucket's residue arenas (K * n elements in
+// each of the A and B arenas).
+struct BatchProd {
+    const uint32_t* a;
+    const uint32_t* b;
+    uint32_t* out;
+    uint32_t la, lb;       // operand words (out receives la + lb words)
+    uint32_t square;       // b is a
+    uint32_t pad;
+    uint64_t res_off;
+    CarryState* cst;       // carry look-back state (4-step buckets)
+    uint4* rec_x;
+    uint32_t* rec_s;
 };
 
 // ------------------------------------------------------------------ helpers
@@ -278,22 +295,17 @@ __device__ __forceinline__ void stage_table(Tw<T>* dst, const Tw<T>* src, int lo
 // tail beyond it is the virtual zero pad.  zt_mask bit z says operand z has
 // all coefficients in the top half of the rows (rows >= R/2 are zero).
 template <class Ar, bool SPLIT16, int RLOG, bool TS>
-__global__ void __launch_bounds__(kColThreads)
-k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
-          const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
-          typename Ar::T* res_b, unsigned zt_mask) {
+__device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
+                                             const uint32_t* __restrict__ limbs, size_t ncoef,
+                                             typename Ar::T* res, bool zt_in, int tile,
+                                             unsigned char* smem_raw) {
     using T = typename Ar::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int op = blockIdx.z;
-    const uint32_t* __restrict__ limbs = op ? limbs_b : limbs_a;
-    const size_t ncoef = op ? ncoef_b : ncoef_a;
-    T* res = op ? res_b : res_a;
-    const bool zt = ((zt_mask >> op) & 1u) && P.log_r > 0;
+    const bool zt = zt_in && P.log_r > 0;
     const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb;
     const int R = 1 << log_r, CB = 1 << log_cb;
     const size_t C = (size_t)1 << log_c;  // stride between rows (R2 * C columns)
     const size_t n = (size_t)R * C;
-    const int c0 = blockIdx.x << log_cb;
+    const int c0 = tile << log_cb;
     const int rows_loaded = zt ? R / 2 : R;
 
     Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
@@ -351,6 +363,34 @@ k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoe
     }
 }
 
+template <class Ar, bool SPLIT16, int RLOG, bool TS>
+__global__ void __launch_bounds__(kColThreads)
+k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
+          const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
+          typename Ar::T* res_b, unsigned zt_mask) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int op = blockIdx.z;
+    fwd_col_body<Ar, SPLIT16, RLOG, TS>(P, op ? limbs_b : limbs_a, op ? ncoef_b : ncoef_a,
+                                        op ? res_b : res_a, (zt_mask >> op) & 1u, blockIdx.x,
+                                        smem_raw);
+}
+
+// batched: blockIdx.z = 2 * product + operand
+template <class Ar, bool SPLIT16, int RLOG>
+__global__ void __launch_bounds__(kColThreads)
+kb_fwd_col(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* res_a,
+           typename Ar::T* res_b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BatchProd d = D[blockIdx.z >> 1];
+    const int op = blockIdx.z & 1;
+    if (op && d.square) return;
+    const size_t ncoef = (size_t)(op ? d.lb : d.la) * (SPLIT16 ? 2 : 1);
+    const size_t n = (size_t)1 << P.log_n;
+    fwd_col_body<Ar, SPLIT16, RLOG, false>(P, op ? d.b : d.a, ncoef,
+                                           (op ? res_b : res_a) + d.res_off, ncoef <= n / 2,
+                                           blockIdx.x, smem_raw);
+}
+
 // ------------------------------------------------------------------ K2
 // Per-row twiddle tables: F[i] = w^(i k1), G[j] = w^(j 2^a k1) (forward) and
 // the inverse pair with n^-1 2^bits folded into Gi.  w^e comes from the
@@ -371,18 +411,16 @@ __device__ __forceinline__ Tw<typename Ar::T> pow_entry(const Ar& ar, uint64_t e
 // C-point NTT, inverse twiddle.  The result overwrites the A row.
 // square: B is A.
 template <class Ar, int NT, int RLOG>
-__global__ void __launch_bounds__(NT)
-k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, int square) {
+__device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* res_a,
+                                         const typename Ar::T* res_b, int square, int prow,
+                                         int kp, unsigned char* smem_raw) {
     using T = typename Ar::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int log_c = P.log_c;
     const int C = 1 << log_c;
     const size_t n = (size_t)1 << P.log_n;  // residues per prime
     // rows come in groups of R_row = 2^log_rr: the last column pass's length
     const int log_rr = P.log_r2 ? P.log_r2 : P.log_r;
     const size_t n_row = (size_t)C << log_rr;  // length of the row-level twiddle
-    const int prow = blockIdx.x;
-    const int kp = blockIdx.y;
     const PrimeDev<Ar>& pr = P.pr[kp];
     const Ar ar = pr.ar;
     T* ga = res_a + (size_t)kp * n + (size_t)prow * C;
@@ -502,6 +540,24 @@ k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, i
     }
 }
 
+template <class Ar, int NT, int RLOG>
+__global__ void __launch_bounds__(NT)
+k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, int square) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    row_body<Ar, NT, RLOG>(P, res_a, res_b, square, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+// batched: blockIdx.z = product
+template <class Ar, int NT, int RLOG>
+__global__ void __launch_bounds__(NT)
+kb_row(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* res_a,
+       const typename Ar::T* res_b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BatchProd d = D[blockIdx.z];
+    row_body<Ar, NT, RLOG>(P, res_a + d.res_off, (d.square ? res_a : res_b) + d.res_off,
+                           d.square, blockIdx.x, blockIdx.y, smem_raw);
+}
+
 // ------------------------------------------------------------------ K1b / K3b
 // Middle column pass of the three-pass schedule (n = R * R2 * C).  Sub-matrix
 // s (blockIdx.y, k1 = bitrev(s) over R) is the contiguous span
@@ -519,7 +575,6 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int log_r2 = P.log_r2, log_c = P.log_c, log_cb = P.log_cb2;
     const int R2 = 1 << log_r2, CB = 1 << log_cb;
-    const size_t C = (size_t)1 << log_c;
     const size_t n = (size_t)1 << P.log_n;
     const int s = blockIdx.y;
     const int kp = blockIdx.z % P.K;
@@ -600,17 +655,16 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
 // fully reduced residues of the cyclic convolution in natural order, in place.
 // Block (0,0) also resets the carry ticket for the K4 launch that follows.
 template <class Ar, int RLOG, bool TS>
-__global__ void __launch_bounds__(kColThreads)
-k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
+__device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::T* res,
+                                             CarryState* cst, int tile, int kp,
+                                             unsigned char* smem_raw) {
     using T = typename Ar::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) cst->counter = 0;
+    if (tile == 0 && kp == 0 && threadIdx.x == 0) cst->counter = 0;
     const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb;
     const int R = 1 << log_r;
     const size_t C = (size_t)1 << log_c;
     const size_t n = (size_t)R * C;
-    const int c0 = blockIdx.x << log_cb;
-    const int kp = blockIdx.y;
+    const int c0 = tile << log_cb;
     const PrimeDev<Ar>& pr = P.pr[kp];
     const Ar ar = pr.ar;
     T* g = res + (size_t)kp * n;
@@ -644,6 +698,23 @@ k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
     }
 }
 
+template <class Ar, int RLOG, bool TS>
+__global__ void __launch_bounds__(kColThreads)
+k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    inv_col_body<Ar, RLOG, TS>(P, res, cst, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+// batched: blockIdx.z = product
+template <class Ar, int RLOG>
+__global__ void __launch_bounds__(kColThreads)
+kb_inv_col(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* res_a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const BatchProd d = D[blockIdx.z];
+    inv_col_body<Ar, RLOG, false>(P, res_a + d.res_off, d.cst, blockIdx.x, blockIdx.y,
+                                  smem_raw);
+}
+
 // ------------------------------------------------------------------ K4
 // Garner + carry.  Output word j of the product collects the "digit sum"
 // D_j (< 2^96): the coefficient j (32-bit coefficients), or coefficients
@@ -667,69 +738,17 @@ k_inv_col(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst) {
 // three-pass carry (src/carry_prop.cu:8-80) with its host-polled fixup loop
 // (src/gpu_ntt.cu:908-924).
 
-// CTA-wide resolution of a 1-bit carry chain.  Each thread has a status
-// st: 0 kill, 1 propagate, 2 generate.  chain_prepare publishes per-warp
-// aggregates (carry out for carry-in 0 / 1) in s_w and must be followed by a
-// __syncthreads(); chain_out gives the CTA carry-out for a carry-in, and
-// chain_mine the carry into the calling thread.
-struct ChainMasks {
-    uint64_t A, B;
-};
-__device__ __forceinline__ ChainMasks chain_prepare(int st, uint32_t* s_w) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t G = __ballot_sync(0xffffffffu, st == 2);
-    const uint32_t Pm = __ballot_sync(0xffffffffu, st == 1);
-    ChainMasks m;
-    m.A = (uint64_t)(G | Pm);
-    m.B = (uint64_t)G;
-    if (lane == 0) {
-        const uint32_t c0 = (uint32_t)((m.A + m.B) >> 32) & 1u;
-        const uint32_t c1 = (uint32_t)((m.A + m.B + 1) >> 32) & 1u;
-        s_w[warp] = c0 | (c1 << 1);
-    }
-    return m;
-}
-__device__ __forceinline__ uint32_t chain_out(const uint32_t* s_w, uint32_t cin) {
-    uint32_t c = cin;
-    const int nw = blockDim.x >> 5;
-    for (int w = 0; w < nw; ++w) c = (s_w[w] >> c) & 1u;
-    return c;
-}
-__device__ __forceinline__ uint32_t chain_mine(const ChainMasks& m, const uint32_t* s_w,
-                                               uint32_t cin) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t ci = cin;
-    for (int w = 0; w < warp; ++w) ci = (s_w[w] >> ci) & 1u;
-    const uint64_t S = m.A + m.B + ci;
-    const uint32_t carries = (uint32_t)(S ^ m.A ^ m.B);
-    return (carries >> lane) & 1u;
-}
-
-template <class Ar, bool SPLIT16>
-__global__ void __launch_bounds__(kCarryThreads)
-k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
-               uint32_t* __restrict__ out, size_t M, size_t NL, CarryState* cst,
-               uint4* __restrict__ rec_x, uint32_t* __restrict__ rec_s, uint32_t epoch,
-               uint32_t wait_epoch, uint32_t* __restrict__ err, int spin_limit) {
+// Garner reconstruction of the E output words starting at word j0: digit
+// sums D[e] < 2^96 (one coefficient per word, or two 16-bit ones).  Words at
+// or beyond NL read nothing and are zero.  Sets *bad when the redundant
+// third prime disagrees or a value reaches 2^96.
+template <class Ar, bool SPLIT16, int E, bool NC = true>
+__device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
+                                              const typename Ar::T* __restrict__ res, size_t n,
+                                              size_t j0, size_t NL, unsigned __int128 (&D)[E],
+                                              uint32_t* bad_out) {
     using T = typename Ar::T;
-    constexpr int E = kCarryWordsPerThread;
-    constexpr int TL = kCarryTileWords;
-    constexpr int CPW = SPLIT16 ? 2 : 1;  // coefficients per output word
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_w[kCarryThreads / 32];
-    __shared__ uint32_t s_lastx[kCarryThreads / 32][3];
-    __shared__ uint32_t s_cin[3];
-    __shared__ uint32_t s_eps;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(&cst->counter, 1u);
-    __syncthreads();
-    const uint32_t t = s_tile;
-    const size_t j0 = (size_t)t * TL + (size_t)tid * E;
-    const size_t n = (size_t)1 << P.log_n;
-
-    // ---- Garner: digit sums D[e] < 2^96
-    unsigned __int128 D[E];
+    constexpr int CPW = SPLIT16 ? 2 : 1;
     uint32_t bad = 0;
     {
         const Ar a1 = P.pr[1].ar;
@@ -748,7 +767,9 @@ k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
                     reinterpret_cast<const uint4*>(res + (size_t)kp * n + j0 * CPW);
 #pragma unroll
                 for (int q = 0; q < (E * CPW * (int)sizeof(T)) / 16; ++q) {
-                    const uint4 v = __ldg(src + q);
+                    // NC: read-only path (residues from an earlier kernel);
+                    // plain loads when this kernel wrote them
+                    const uint4 v = NC ? __ldg(src + q) : src[q];
                     if constexpr (sizeof(T) == 8) {
                         r[kp][2 * q] = ((uint64_t)v.y << 32) | v.x;
                         r[kp][2 * q + 1] = ((uint64_t)v.w << 32) | v.z;
@@ -792,6 +813,73 @@ k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
             bad |= (uint32_t)((D[e] >> 96) != 0);
         }
     }
+    *bad_out |= bad;
+}
+
+// CTA-wide resolution of a 1-bit carry chain.  Each thread has a status
+// st: 0 kill, 1 propagate, 2 generate.  chain_prepare publishes per-warp
+// aggregates (carry out for carry-in 0 / 1) in s_w and must be followed by a
+// __syncthreads(); chain_out gives the CTA carry-out for a carry-in, and
+// chain_mine the carry into the calling thread.
+struct ChainMasks {
+    uint64_t A, B;
+};
+__device__ __forceinline__ ChainMasks chain_prepare(int st, uint32_t* s_w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t G = __ballot_sync(0xffffffffu, st == 2);
+    const uint32_t Pm = __ballot_sync(0xffffffffu, st == 1);
+    ChainMasks m;
+    m.A = (uint64_t)(G | Pm);
+    m.B = (uint64_t)G;
+    if (lane == 0) {
+        const uint32_t c0 = (uint32_t)((m.A + m.B) >> 32) & 1u;
+        const uint32_t c1 = (uint32_t)((m.A + m.B + 1) >> 32) & 1u;
+        s_w[warp] = c0 | (c1 << 1);
+    }
+    return m;
+}
+__device__ __forceinline__ uint32_t chain_out(const uint32_t* s_w, uint32_t cin) {
+    uint32_t c = cin;
+    const int nw = blockDim.x >> 5;
+    for (int w = 0; w < nw; ++w) c = (s_w[w] >> c) & 1u;
+    return c;
+}
+__device__ __forceinline__ uint32_t chain_mine(const ChainMasks& m, const uint32_t* s_w,
+                                               uint32_t cin) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t ci = cin;
+    for (int w = 0; w < warp; ++w) ci = (s_w[w] >> ci) & 1u;
+    const uint64_t S = m.A + m.B + ci;
+    const uint32_t carries = (uint32_t)(S ^ m.A ^ m.B);
+    return (carries >> lane) & 1u;
+}
+
+template <class Ar, bool SPLIT16>
+__device__ __forceinline__ void garner_carry_body(
+    const PlanDev<Ar>& P, const typename Ar::T* __restrict__ res, uint32_t* __restrict__ out,
+    size_t M, size_t NL, CarryState* cst, uint4* __restrict__ rec_x,
+    uint32_t* __restrict__ rec_s, uint32_t epoch, uint32_t wait_epoch,
+    uint32_t* __restrict__ err, int spin_limit) {
+    using T = typename Ar::T;
+    constexpr int E = kCarryWordsPerThread;
+    constexpr int TL = kCarryTileWords;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_w[kCarryThreads / 32];
+    __shared__ uint32_t s_lastx[kCarryThreads / 32][3];
+    __shared__ uint32_t s_cin[3];
+    __shared__ uint32_t s_eps;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(&cst->counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const size_t j0 = (size_t)t * TL + (size_t)tid * E;
+    const size_t n = (size_t)1 << P.log_n;
+
+    // ---- Garner: digit sums D[e] < 2^96
+    unsigned __int128 D[E];
+    uint32_t bad = 0;
+    garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
     if (bad) atomicOr(err, 2u);
 
     // ---- local carry: words l[0..E) and carry-out X < 2^66
@@ -937,6 +1025,232 @@ k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
         for (int e = 0; e < E; ++e)
             if (j0 + e < M) out[j0 + e] = w[e];
     }
+}
+
+template <class Ar, bool SPLIT16>
+__global__ void __launch_bounds__(kCarryThreads)
+k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
+               uint32_t* __restrict__ out, size_t M, size_t NL, CarryState* cst,
+               uint4* __restrict__ rec_x, uint32_t* __restrict__ rec_s, uint32_t epoch,
+               uint32_t wait_epoch, uint32_t* __restrict__ err, int spin_limit) {
+    garner_carry_body<Ar, SPLIT16>(P, res, out, M, NL, cst, rec_x, rec_s, epoch, wait_epoch, err,
+                                   spin_limit);
+}
+
+// batched: blockIdx.y = product
+template <class Ar, bool SPLIT16>
+__global__ void __launch_bounds__(kCarryThreads)
+kb_garner_carry(const PlanDev<Ar> P, const BatchProd* __restrict__ D,
+                const typename Ar::T* __restrict__ res_a, uint32_t epoch,
+                uint32_t* __restrict__ err, int spin_limit) {
+    const BatchProd d = D[blockIdx.y];
+    const size_t NL = ((size_t)1 << P.log_n) / (SPLIT16 ? 2 : 1);
+    garner_carry_body<Ar, SPLIT16>(P, res_a + d.res_off, d.out, (size_t)d.la + d.lb, NL, d.cst,
+                                   d.rec_x, d.rec_s, epoch, epoch, err, spin_limit);
+}
+
+// ------------------------------------------------------------------ small products
+// One CTA computes a whole product whose n-point transform fits in shared
+// memory (a batch bucket of equal n, blockIdx.x = product): for each prime
+// the forward transforms of both operands, the pointwise product and the
+// inverse transform run in shared memory (stage twiddles pr.WCf / pr.WCi of
+// length n, scale pr.scale = n^-1 2^bits), the residues go to a per-product
+// global scratch (L2-resident at these sizes); then Garner + carry over the
+// product's words in tiles of NT*8 words, the carry handed from tile to tile
+// inside the CTA, so no look-back is needed.
+template <class Ar, bool SPLIT16, int NT>
+__global__ void __launch_bounds__(NT)
+ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* scratch,
+           uint32_t* __restrict__ err) {
+    using T = typename Ar::T;
+    constexpr int RLOG = 4;
+    constexpr int E = kCarryWordsPerThread;
+    constexpr int CPW = SPLIT16 ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t s_w[NT / 32];
+    __shared__ uint32_t s_lastx[NT / 32][3];
+    __shared__ uint32_t s_cin[3];
+    __shared__ uint32_t s_eps;
+    const BatchProd d = D[blockIdx.x];
+    const int log_n = P.log_n;
+    const int n = 1 << log_n;
+    T* bufA = reinterpret_cast<T*>(smem_raw);
+    T* bufB = bufA + n;
+    T* res = scratch + d.res_off;
+    const size_t nca = (size_t)d.la * CPW, ncb = (size_t)d.lb * CPW;
+    const int sq = d.square;
+    const int nr = sched_rounds<RLOG>(log_n);
+    auto coef = [&](const uint32_t* src, size_t nc, int i) -> T {
+        if ((size_t)i >= nc) return T(0);
+        if constexpr (SPLIT16) {
+            return (T)((__ldg(src + (i >> 1)) >> ((i & 1) * 16)) & 0xFFFFu);
+        } else {
+            return (T)__ldg(src + i);
+        }
+    };
+    auto ldA = [&](int, int idx) -> T { return bufA[swz<T>(idx)]; };
+
+    for (int kp = 0; kp < P.K; ++kp) {
+        const PrimeDev<Ar>& pr = P.pr[kp];
+        const Ar ar = pr.ar;
+        const Tw<T> sc = pr.scale;
+        auto st_res = [&](int idx, T v) {
+            res[(size_t)kp * n + idx] = ar.red1(ar.shoup(v, sc.w, sc.wq));
+        };
+        for (int i = threadIdx.x; i < n; i += NT) {
+            bufA[swz<T>(i)] = coef(d.a, nca, i);
+            if (!sq) bufB[swz<T>(i)] = coef(d.b, ncb, i);
+        }
+        __syncthreads();
+        for (int op = 0; op < (sq ? 1 : 2); ++op) {
+            T* buf = op ? bufB : bufA;
+            const int rounds = (op == 0 && !sq) ? nr : nr - 1;
+            auto ld = [&](int, int idx) -> T { return buf[swz<T>(idx)]; };
+            auto st = [&](int, int idx, T v) { buf[swz<T>(idx)] = v; };
+            for (int r = 0; r < rounds; ++r) {
+                run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
+                                                     sched_s0<RLOG>(log_n, r), pr.WCf, ar, false,
+                                                     ld, st);
+                __syncthreads();
+            }
+        }
+        {
+            // last forward round of B (or A), product, first inverse round
+            const int r = nr - 1;
+            const int rl = sched_rl<RLOG>(log_n, r), s0 = sched_s0<RLOG>(log_n, r);
+            const int d_log = log_n - s0 - rl;
+            const int nsub = 1 << (log_n - rl);
+            const bool final_round = (nr == 1);
+            T* src = sq ? bufA : bufB;
+            for (int sp = threadIdx.x; sp < nsub; sp += NT) {
+                const int j = sp & ((1 << d_log) - 1);
+                const int g = sp >> d_log;
+                const int base = (g << (d_log + rl)) + j;
+                T x[1 << RLOG];
+#define BW_SMALL_FUSED(RL)                                                             \
+    {                                                                                  \
+        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] =                   \
+            src[swz<T>(base + (k << d_log))];                                          \
+        ct_stages<Ar, RL, false>(x, s0, g, pr.WCf, ar, false);                         \
+        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
+            const T xa = ar.fwd_to_2p(x[k]);                                           \
+            const T ya = sq ? xa : ar.fwd_to_2p(bufA[swz<T>(base + (k << d_log))]);    \
+            x[k] = ar.mont(xa, ya);                                                    \
+        }                                                                              \
+        gs_stages<Ar, RL, false>(x, s0, g, pr.WCi, ar);                                \
+        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
+            const int idx = base + (k << d_log);                                       \
+            if (final_round) st_res(idx, x[k]); else bufA[swz<T>(idx)] = x[k];         \
+        }                                                                              \
+    }
+                if (rl == RLOG) {
+                    BW_SMALL_FUSED(RLOG)
+                } else if (rl == 3) {
+                    BW_SMALL_FUSED(3)
+                } else if (rl == 2) {
+                    BW_SMALL_FUSED(2)
+                } else {
+                    BW_SMALL_FUSED(1)
+                }
+#undef BW_SMALL_FUSED
+            }
+            __syncthreads();
+        }
+        for (int r = nr - 2; r >= 0; --r) {
+            const bool last = (r == 0);
+            auto st = [&](int, int idx, T v) {
+                if (last) {
+                    st_res(idx, v);
+                } else {
+                    bufA[swz<T>(idx)] = v;
+                }
+            };
+            run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
+                                                sched_s0<RLOG>(log_n, r), pr.WCi, ar, false, ldA,
+                                                st);
+            __syncthreads();
+        }
+    }
+
+    // ---- Garner + carry, tile by tile; the carry into a tile is the previous
+    // tile's last carry words (s_cin) plus its chain carry-out bit (s_eps)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t NL = (size_t)n / CPW, M = (size_t)d.la + d.lb;
+    const size_t words = NL > M ? NL : M;
+    if (tid == 0) {
+        s_cin[0] = s_cin[1] = s_cin[2] = 0;
+        s_eps = 0;
+    }
+    __syncthreads();
+    uint32_t bad = 0;
+    for (size_t t0 = 0; t0 < words; t0 += (size_t)NT * E) {
+        const size_t j0 = t0 + (size_t)tid * E;
+        unsigned __int128 Dg[E];
+        garner_digits<Ar, SPLIT16, E, false>(P, res, n, j0, NL, Dg, &bad);
+        uint32_t l[E], X[3];
+        {
+            unsigned __int128 acc = 0;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                acc += Dg[e];
+                l[e] = (uint32_t)acc;
+                acc >>= 32;
+            }
+            X[0] = (uint32_t)acc;
+            X[1] = (uint32_t)(acc >> 32);
+            X[2] = (uint32_t)(acc >> 64);
+        }
+        uint32_t PX[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) PX[q] = __shfl_up_sync(0xffffffffu, X[q], 1);
+        if (lane == 31) {
+            s_lastx[warp][0] = X[0];
+            s_lastx[warp][1] = X[1];
+            s_lastx[warp][2] = X[2];
+        }
+        __syncthreads();
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) PX[q] = warp > 0 ? s_lastx[warp - 1][q] : s_cin[q];
+        }
+        uint32_t S[E];
+        int st;
+        {
+            uint64_t c = 0;
+            uint32_t all = 0xffffffffu;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const uint64_t s = (uint64_t)l[e] + (e < 3 ? PX[e] : 0u) + c;
+                S[e] = (uint32_t)s;
+                c = s >> 32;
+                all &= S[e];
+            }
+            st = c ? 2 : (all == 0xffffffffu ? 1 : 0);
+        }
+        const ChainMasks cm = chain_prepare(st, s_w);
+        __syncthreads();
+        const uint32_t eps_in = s_eps;
+        const uint32_t mc = chain_mine(cm, s_w, eps_in);
+        const uint32_t cout = chain_out(s_w, eps_in);
+        {
+            uint64_t c = mc;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const uint64_t s = (uint64_t)S[e] + c;
+                if (j0 + e < M) d.out[j0 + e] = (uint32_t)s;
+                c = s >> 32;
+            }
+        }
+        __syncthreads();  // every thread has read s_cin, s_eps, s_lastx, s_w
+        if (tid == NT - 1) {
+            s_cin[0] = X[0];
+            s_cin[1] = X[1];
+            s_cin[2] = X[2];
+        }
+        if (tid == 0) s_eps = cout;
+        __syncthreads();
+    }
+    if (bad) atomicOr(err, 2u);
 }
 
 }  // namespace bw

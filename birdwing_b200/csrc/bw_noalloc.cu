@@ -17,6 +17,7 @@
 // pointer is what the kernel receives.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -120,7 +121,9 @@ int run(int path, int K, const void* residues, size_t n, int log_n, uint32_t* ou
         size_t out_words, cudaStream_t s) {
     using T = typename Ar::T;
     const size_t NL = n / (SPLIT16 ? 2 : 1);
-    const size_t ntiles = (NL + kCarryTileWords - 1) / kCarryTileWords;
+    // one word beyond the coefficients can hold the final carry
+    const size_t words = std::max(NL, std::min(out_words, NL + 1));
+    const size_t ntiles = (words + kCarryTileWords - 1) / kCarryTileWords;
     if (ntiles > (size_t)BW_NOALLOC_MAX_TILES)
         return bw_fail(BW_ESIZE,
                        "bw_garner_carry_noalloc: %zu output words need %zu carry tiles, the "

@@ -210,8 +210,9 @@ int bw_ctx_inject_wait_fault(bw_ctx* ctx, int enable);
  * arrays of n fully reduced residues, array k at residues + k * n elements,
  * u64 elements for BW_PATH_P64 and u32 for BW_PATH_P32, in natural
  * coefficient order, exactly as the library's own pipeline leaves them.  It
- * writes out[0 .. min(out_words, n / c)) with c = 1 (P64) or 2 (P32: two
- * 16-bit coefficients per word).  The primes are the library's, see
+ * writes out[0 .. min(out_words, n / c + 1)) with c = 1 (P64) or 2 (P32: two
+ * 16-bit coefficients per word); word n / c, when asked for, receives the
+ * final carry.  The primes are the library's, see
  * bw_plan_get_info.  n is a power of two >= 16 and n / c is at most
  * BW_NOALLOC_MAX_TILES * 2048, else BW_ESIZE.  The look-back scratch is one
  * fixed-size device array in the library (about 640 KiB on every GPU that
@@ -231,6 +232,130 @@ int bw_garner_carry_noalloc(int path, int num_primes, const void* residues, size
 int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b,
                           size_t lb, uint32_t* c, size_t lc, int path,
                           float* elapsed_ms);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent products of uneven sizes in one launch sequence.  The
+ * reference has no batched form (each product is one host_multiply_merge
+ * call, src/host_multiply.cpp:27-86); these calls add it.
+ *
+ * Products are grouped by transform length; each group runs as one set of
+ * kernels over all of its products (small groups: one CTA per whole
+ * product; larger ones: the 4-step kernels with a product grid dimension).
+ * The groups run concurrently inside one CUDA graph that is replayed for as
+ * long as the list of products (their sizes) stays the same.  Transform
+ * lengths up to 2^26 (P64: products of up to 2^26 words; P32: 2^25, within
+ * the path's own limit). */
+typedef struct bw_batch bw_batch;
+
+#define BW_BATCH_THREE_PRIMES 1u  /* bw_batch_create: K = 3 (redundant check) */
+
+/* bw_batch_run `what` bits (0 = all three) */
+#define BW_BATCH_UPLOAD 1u    /* copy every product's operands to the device */
+#define BW_BATCH_COMPUTE 2u   /* run the products */
+#define BW_BATCH_DOWNLOAD 4u  /* copy every result back to its host buffer */
+
+typedef struct {
+    size_t products;
+    size_t buckets;        /* groups of equal transform length */
+    size_t small_buckets;  /* groups run one CTA per product */
+    size_t graph_nodes;    /* nodes of the captured graph */
+    size_t device_bytes;   /* device memory the batch holds */
+} bw_batch_info;
+
+/* stream = NULL creates a private stream. */
+int bw_batch_create(bw_batch** out, void* stream, unsigned flags);
+int bw_batch_destroy(bw_batch* batch);
+/* Forget every product (the device buffers are kept for reuse). */
+int bw_batch_clear(bw_batch* batch);
+/* Append c[0 .. la+lb) = a * b (host pointers, read at every run with
+ * BW_BATCH_UPLOAD; c written at every run with BW_BATCH_DOWNLOAD).
+ * a == b with la == lb squares.  path BW_PATH_AUTO means P64. */
+int bw_batch_add(bw_batch* batch, int path, const uint32_t* a, size_t la,
+                 const uint32_t* b, size_t lb, uint32_t* c, size_t lc);
+/* Run the batch (blocking).  The first run after bw_batch_add/clear builds
+ * the groups and captures the graph.  timing gets h2d_ms, mul_ms, d2h_ms and
+ * total_ms.  BW_ECHECK / BW_ETIMEOUT as for bw_multiply. */
+int bw_batch_run(bw_batch* batch, unsigned what, bw_timing* timing);
+int bw_batch_get_info(const bw_batch* batch, bw_batch_info* info);
+
+/* Time each candidate form of each group (one CTA per product where the
+ * transform fits shared memory; 4-step with three column/row splits) on the
+ * batch's own products, `reps` runs each, and keep the fastest in the
+ * process-wide tune table that later layouts use.  Blocking. */
+int bw_batch_autotune(bw_batch* batch, int reps);
+/* The tune table as a JSON array of {path, num_primes, log_n, small,
+ * log_cols, ms}.  Writes at most len bytes including the terminating NUL;
+ * *needed gets the full size. */
+int bw_tune_table_export(char* buf, size_t len, size_t* needed);
+/* Set one tune-table entry (log_cols 0 = automatic split). */
+int bw_tune_table_set(int path, int num_primes, int log_n, int small, int log_cols);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop with continuous batching.  Requests (host buffers) are
+ * submitted from any thread as they arrive and finish asynchronously.  Two
+ * library threads run the loop: one admits waiting requests in arrival
+ * order while the device bytes they need fit the budget, groups them by
+ * transform length and issues each group as one batched launch on one of
+ * several streams (at most max_groups_in_flight groups on the device; what
+ * arrives meanwhile is admitted together into the next groups); the other
+ * detects finished groups, copies results out and frees their memory.
+ * Twiddle tables stay resident between requests.  No reference counterpart:
+ * the reference multiplies one product per blocking host_multiply_merge call
+ * (src/host_multiply.cpp:27-86). */
+typedef struct bw_server bw_server;
+
+typedef struct bw_server_config {
+    size_t   hbm_budget_bytes;      /* admission budget: resident tables +
+                                       in-flight groups (0 = 120 GiB)       */
+    size_t   pinned_bytes;          /* host staging (0 = 2 GiB)             */
+    int      lanes;                 /* streams groups are issued on (0 = 8) */
+    int      max_groups_in_flight;  /* (0 = 2 * lanes)                      */
+    int      num_primes;            /* K (0 = 2)                            */
+    int      path;                  /* default path (BW_PATH_AUTO = P64)    */
+} bw_server_config;
+
+/* One finished request.  Times are microseconds on a steady clock since the
+ * server was created; admit/launch are -1 for a request that never ran. */
+typedef struct bw_request_info {
+    uint64_t ticket;
+    int      status;        /* BW_OK, or why the request failed            */
+    double   submit_us, admit_us, launch_us, done_us;
+    size_t   group_size;    /* products in the launch group it ran in      */
+    size_t   device_bytes;  /* bytes charged against the budget            */
+    size_t   la, lb;
+} bw_request_info;
+
+typedef struct bw_server_stats {
+    uint64_t submitted, completed, rejected, failed;
+    uint64_t groups, kernel_launches;
+    size_t   max_group_size;
+    size_t   bytes_in_flight, peak_bytes_in_flight;  /* incl. resident tables */
+    size_t   resident_plan_bytes, queue_depth, groups_in_flight, budget_bytes;
+} bw_server_stats;
+
+/* cfg may be NULL (all defaults).  Uses the current CUDA device. */
+int bw_server_create(bw_server** out, const bw_server_config* cfg);
+/* Waiting requests fail with BW_EBUSY; admitted ones finish first. */
+int bw_server_destroy(bw_server* server);
+/* Build the resident tables for every transform length up to 2^max_log_n. */
+int bw_server_prewarm(bw_server* server, int path, int max_log_n);
+/* Queue c[0 .. la+lb) = a * b.  a, b and c must stay valid until the
+ * request finishes.  a == b with la == lb squares.  BW_EREJECT when the
+ * request alone needs more than the budget; BW_ESIZE beyond the limits
+ * (transform length 2^26 at most). */
+int bw_server_submit(bw_server* server, int path, const uint32_t* a, size_t la,
+                     const uint32_t* b, size_t lb, uint32_t* c, size_t lc,
+                     uint64_t* ticket);
+/* Wait for one request (timeout_ms < 0: no limit; 0: poll) and release it.
+ * Returns its status, or BW_ETIMEOUT if it has not finished. */
+int bw_server_wait(bw_server* server, uint64_t ticket, int timeout_ms,
+                   bw_request_info* info);
+/* Take up to max finished requests (any order) and release them. */
+int bw_server_harvest(bw_server* server, bw_request_info* out, size_t max,
+                      size_t* count);
+/* Wait until nothing is waiting or running. */
+int bw_server_drain(bw_server* server, int timeout_ms);
+int bw_server_get_stats(bw_server* server, bw_server_stats* out);
 
 #ifdef __cplusplus
 }
