@@ -58,25 +58,40 @@ BATCH_CONFIGS = {
     "3prof": (512, 3, 2, "batched uneven sizes, 512 products of the same mix"),
 }
 
+# serving configurations: (distinct requests in the pool, seed, K, description)
+SERVE_CONFIGS = {
+    "5": (1024, 5, 2,
+          "serving: open-loop Poisson arrivals, operands 2^10..2^24 bits log-uniform, 20% "
+          "squarings, second operand 1/8x..1x, 64-bit path, 2 primes, 120 GiB admission budget"),
+}
+
 
 def parse():
+    return parse_args_list(None)
+
+
+def parse_args_list(argv):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS))
+    ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--autotune", action="store_true",
                     help="batched configurations: tune each bucket's kernel form first")
     ap.add_argument("--no-plain", action="store_true",
-                    help="batched configurations: skip the plain per-product loop")
+                    help="batched/serving configurations: skip the plain per-product path")
+    ap.add_argument("--duration", type=float, default=10.0,
+                    help="serving: seconds of arrivals per swept rate")
+    ap.add_argument("--rate-fracs", default="0.3,0.6,0.85",
+                    help="serving: arrival rates as fractions of the closed-loop capacity")
     ap.add_argument("--log-cols", type=int, default=0,
                     help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")
     ap.add_argument("--plan-flags", type=lambda s: int(s, 0), default=0,
                     help="extra bw_plan_create flags (tuning switches)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def operands(cfg, rank):
@@ -116,6 +131,29 @@ def load_traffic(cfg, kernel):
             return json.load(f)[cfg][kernel]
     except Exception:
         return None
+
+
+def reduce_over_ranks(values, ops):
+    """All-reduce one float per entry across the job's ranks: "max" for times
+    (the slowest rank bounds the job), "sum" for counts.  A no-op on a single
+    process.  Runs on the GPU under NCCL and on the CPU under gloo."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    out = []
+    for v, op in zip(values, ops):
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        out.append(float(t.item()))
+    return out
+
+
+def job_throughput(units_per_rank, world, rank_ms):
+    """Whole-job units/s: every rank processed units_per_rank units and the
+    job took the slowest rank's time (ms, already reduced with max)."""
+    return world * units_per_rank / (rank_ms * 1e-3)
 
 
 class ClockSampler:
@@ -301,10 +339,7 @@ def bench_batch(args):
             dist.barrier()
 
     def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks([x], ["max"])[0]
 
     items, K = batch_items(args.config, rank)
     count, _, _, desc = BATCH_CONFIGS[args.config]
@@ -415,7 +450,7 @@ def bench_batch(args):
         h2d = sum(4 * (len(a) + len(b)) for _, a, b in items)
         d2h = sum(4 * (len(a) + len(b)) for _, a, b in items) + 4
         line = {
-            "metric": "products/s", "value": world * count * args.steps / (total_ms * 1e-3),
+            "metric": "products/s", "value": job_throughput(count * args.steps, world, total_ms),
             "unit": "products/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64/u32", "data": "synthetic",
@@ -487,8 +522,246 @@ def run_reference_batch(args):
     print(json.dumps(line))
 
 
+def serving_pool(count, seed, rank):
+    """Distinct requests of the serving mix (operand pairs; squarings share
+    one array)."""
+    from birdwing_b200 import workloads
+    rng = np.random.default_rng(seed + 1000 + 100 * rank)
+    pool = []
+    for la, lb, sq in workloads.serving_sizes(count, seed=seed + 100 * rank):
+        a = workloads.rand_operand(rng, la)
+        pool.append((a, a if sq else workloads.rand_operand(rng, lb)))
+    return pool
+
+
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def run_open_loop(srv, pool, expect, rate, duration, seed):
+    """Poisson arrivals at `rate` requests/s for `duration` seconds, cycling
+    through the pool.  Latency = done - submit (library clock); every 8th
+    result is compared with GMP's as it is harvested."""
+    rng = np.random.default_rng(seed)
+    n_arr = int(rate * duration * 1.2) + 16
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_arr))
+    arrivals = arrivals[arrivals < duration]
+    spare = {}                                  # pool index -> free output buffers
+    owner = {}                                  # ticket -> (pool index, buffer, check)
+    lat, late, groups, bad, checked, done_in_window = [], [], [], 0, 0, 0
+    t0 = time.perf_counter()
+
+    def take_finished():
+        nonlocal bad, checked, done_in_window
+        for d in srv.harvest(8192):
+            i, out, chk = owner.pop(d["ticket"])
+            if d["status"] != 0:
+                bad += 1
+            elif chk:
+                checked += 1
+                if not np.array_equal(out, expect[i]):
+                    bad += 1
+            lat.append((d["done_us"] - d["submit_us"]) * 1e-3)
+            groups.append(d["group_size"])
+            if time.perf_counter() - t0 <= duration:
+                done_in_window += 1
+            spare.setdefault(i, []).append(out)
+
+    for k, t_arr in enumerate(arrivals):
+        while True:
+            now = time.perf_counter() - t0
+            if now >= t_arr:
+                break
+            if t_arr - now > 2e-4:
+                take_finished()
+        i = k % len(pool)
+        a, b = pool[i]
+        free = spare.get(i)
+        out = free.pop() if free else np.empty(len(a) + len(b), dtype=np.uint32)
+        late.append((time.perf_counter() - t0 - t_arr) * 1e3)
+        owner[srv.submit(a, b, out=out)] = (i, out, k % 8 == 0)
+    srv.drain()
+    take_finished()
+    wall = time.perf_counter() - t0
+    return {"rate": rate, "submitted": len(arrivals), "completed": len(lat), "bad": bad,
+            "checked_vs_gmp": checked, "submit_late_p99_ms": percentile(late, 99),
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+            "mean_ms": float(np.mean(lat)) if lat else None,
+            "mean_group_size": float(np.mean(groups)) if groups else None,
+            "products_per_s": len(lat) / wall, "drain_s": wall - duration,
+            "completed_in_window": done_in_window}
+
+
+def run_plain_open_loop(pool, rate, duration, seed, max_wall):
+    """The plain per-request path on the same arrival process: one thread
+    serves requests in arrival order with bw_multiply_host_once (plan,
+    context, multiply, teardown -- the drop-in host_multiply_merge).  Requests
+    not served by max_wall count with their waiting time so far."""
+    import ctypes
+
+    from birdwing_b200 import _lib as L
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * duration * 1.2) + 16))
+    arrivals = arrivals[arrivals < duration]
+    lat, unserved = [], 0
+    ms = ctypes.c_float()
+    t0 = time.perf_counter()
+    for k, t_arr in enumerate(arrivals):
+        now = time.perf_counter() - t0
+        if now < t_arr:
+            time.sleep(t_arr - now)
+            now = time.perf_counter() - t0
+        if now > max_wall:
+            unserved = len(arrivals) - k
+            lat.extend((now - arrivals[k:]) * 1e3)
+            break
+        a, b = pool[k % len(pool)]
+        out = np.empty(len(a) + len(b), dtype=np.uint32)
+        L.check(L.lib.bw_multiply_host_once(
+            ctypes.c_void_p(a.ctypes.data), a.size, ctypes.c_void_p(b.ctypes.data), b.size,
+            ctypes.c_void_p(out.ctypes.data), out.size, L.BW_PATH_AUTO, ctypes.byref(ms)))
+        lat.append((time.perf_counter() - t0 - t_arr) * 1e3)
+    wall = time.perf_counter() - t0
+    served = len(arrivals) - unserved
+    return {"rate": rate, "submitted": len(arrivals), "served": served,
+            "unserved_at_cutoff": unserved, "p50_ms": percentile(lat, 50),
+            "p99_ms": percentile(lat, 99), "products_per_s": served / wall,
+            "how": "bw_multiply_host_once per request (plan + context + multiply + teardown), "
+                   "one server thread, arrival order"}
+
+
+def bench_serving(args):
+    import torch
+    import torch.distributed as dist
+
+    import birdwing_b200 as bw
+    from oracle import gmp_ref
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    pool_n, seed, K, desc = SERVE_CONFIGS[args.config]
+    pool = serving_pool(pool_n, seed, rank)
+    expect = [gmp_ref.mul(a, b) for a, b in pool]
+    srv = bw.Server(num_primes=K)
+    srv.prewarm(21)
+    # warm-up: the whole pool, closed loop; the first pass checks every
+    # result against GMP
+    pool_ok = True
+    for w in range(max(1, min(args.warmup, 3))):
+        ts = {srv.submit(a, b): i for i, (a, b) in enumerate(pool)}
+        srv.drain()
+        for d in srv.harvest(len(ts) + 16):
+            if w == 0:
+                pool_ok &= d["status"] == 0 and bool(
+                    np.array_equal(d["out"], expect[ts[d["ticket"]]]))
+    # capacity: the pool submitted at once, twice
+    t0 = time.perf_counter()
+    for _ in range(2):
+        for a, b in pool:
+            srv.submit(a, b)
+        srv.drain()
+        srv.harvest(len(pool) + 16)
+    cap = 2 * len(pool) / (time.perf_counter() - t0)
+    fracs = [float(x) for x in args.rate_fracs.split(",")]
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    sampler.start()
+    st0 = srv.stats()
+    sweep = [run_open_loop(srv, pool, expect, f * cap, args.duration, seed + 7 + j)
+             for j, f in enumerate(fracs)]
+    clocks = sampler.stop()
+    st = srv.stats()
+    srv.close()
+    plain = None
+    if not args.no_plain:
+        plain = run_plain_open_loop(pool, fracs[0] * cap, min(args.duration, 10.0), seed + 99,
+                                    max_wall=2 * min(args.duration, 10.0))
+    # headline: the highest swept rate the server sustained (everything
+    # submitted finished within 10% of the window after it closed)
+    ok = [r for r in sweep if r["bad"] == 0 and r["drain_s"] <= 0.1 * args.duration]
+    head = max(ok, key=lambda r: r["rate"]) if ok else sweep[0]
+    vals = reduce_over_ranks([head["products_per_s"], head["p99_ms"] or 0.0], ["sum", "max"])
+    if rank == 0:
+        mean_in = float(np.mean([4 * (len(a) + (0 if a is b else len(b))) for a, b in pool]))
+        mean_out = float(np.mean([4 * (len(a) + len(b)) for a, b in pool]))
+        line = {
+            "metric": "products/s", "value": vals[0], "unit": "products/s",
+            "n_gpus": world, "steps": head["completed"], "warmup": args.warmup,
+            "ms_per_step": 1000.0 / vals[0], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"config {args.config}: {desc}", "pool": pool_n,
+                       "num_primes": K, "duration_s": args.duration,
+                       "rates": [r["rate"] for r in sweep], "capacity_closed_loop": cap,
+                       "l2": "operands streamed from host per request",
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": head["p50_ms"], "p99": vals[1], "at_rate": head["rate"]},
+            "sweep": sweep,
+            "server_stats": st,
+            "plain_per_request": plain,
+            "correct_vs_gmp": pool_ok and all(r["bad"] == 0 for r in sweep),
+            "e2e": {"value": vals[0], "unit": "products/s",
+                    "h2d_bytes_per_step": mean_in, "d2h_bytes_per_step": mean_out,
+                    "note": "every request is host buffers in, host buffers out"},
+            "gpu_launches": st["kernel_launches"] - st0["kernel_launches"],
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_items([(64, a, b) for a, b in pool], K)
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference_serving(args):
+    """--impl reference on the serving configuration: the oracle serves the
+    request pool in order on all host threads (a bounded sample)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    pool_n, seed, K, desc = SERVE_CONFIGS[args.config]
+    pool = serving_pool(pool_n, seed, 0)
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    lat, t0 = [], time.perf_counter()
+    for a, b in pool:
+        t1 = time.perf_counter()
+        oracle.multiply(a, b, 64, K)
+        lat.append((time.perf_counter() - t1) * 1e3)
+        if time.perf_counter() - t0 >= 120.0:
+            break
+    dt = time.perf_counter() - t0
+    v = len(lat) / dt
+    line = {
+        "impl": "reference", "metric": "products/s", "value": v, "unit": "products/s",
+        "n_gpus": args.gpus, "steps": len(lat), "warmup": 0, "ms_per_step": 1000.0 / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic", "config": {"workload": f"config {args.config}: {desc}",
+                                        "pool": pool_n, "num_primes": K},
+        "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
+                       "note": "service time per request, closed loop (no queueing)"},
+        "cpu_baseline": {"value": v, "unit": "products/s", "cores": cores, "kind": "port",
+                         "sample": f"first {len(lat)} of {pool_n} pool requests, "
+                                   f"oracle/bw_oracle.c on {cores} threads, {dt:.1f} s"},
+        "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.config in SERVE_CONFIGS:
+        if args.impl == "reference":
+            run_reference_serving(args)
+        else:
+            bench_serving(args)
+        return
     if args.config in BATCH_CONFIGS:
         if args.impl == "reference":
             run_reference_batch(args)
@@ -569,10 +842,7 @@ def main():
     for i in range(args.steps):
         per_step.append(ev0[i].elapsed_time(ev1[i]))
     total_ms = sum(per_step)
-    t_max = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    total_ms = float(t_max.item())
+    total_ms = reduce_over_ranks([total_ms], ["max"])[0]
 
     # end to end through the C ABI with pinned host buffers
     ha = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
@@ -586,10 +856,7 @@ def main():
         t0 = time.perf_counter()
         ctx.multiply(ha, hb, out=hc)
         e2e_ms.append(1000 * (time.perf_counter() - t0))
-    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_total = float(e2e_t.item())
+    e2e_total = reduce_over_ranks([sum(e2e_ms)], ["max"])[0]
 
     if rank == 0:
         ms = total_ms / args.steps
@@ -602,7 +869,7 @@ def main():
         achieved = mb[dom] / (means[dom] * 1e-3) / 1e9
         total_model = sum(mb.values())
         line = {
-            "metric": "products/s", "value": world * args.steps / (total_ms * 1e-3),
+            "metric": "products/s", "value": job_throughput(args.steps, world, total_ms),
             "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64" if path == 64 else "u32", "data": "synthetic",

@@ -23,7 +23,7 @@ from ._lib import BwError, check, lib
 __all__ = [
     "Plan", "Context", "host_multiply_merge", "host_multiply_merge_native", "multiply",
     "square", "limits", "size_supported", "int_to_limbs", "limbs_to_int", "BwError", "Batch",
-    "tune_table", "set_tune_entry", "load_tune_table",
+    "tune_table", "set_tune_entry", "load_tune_table", "Server",
 ]
 
 
@@ -312,3 +312,88 @@ def load_tune_table(entries):
     """Install entries as produced by tune_table() (e.g. read back from JSON)."""
     for e in entries:
         set_tune_entry(e["path"], e["num_primes"], e["log_n"], e["small"], e["log_cols"])
+
+
+class Server:
+    """Request loop with continuous batching (bw_server_*).
+
+    ``submit`` queues a product and returns a ticket at once; the library's
+    own threads admit requests by device bytes, batch the ones that wait
+    together, and finish them asynchronously.  The operand and output arrays
+    are kept referenced here until the request is waited for or harvested.
+    """
+
+    def __init__(self, hbm_budget=0, pinned=0, lanes=0, max_groups=0, num_primes=2,
+                 path=L.BW_PATH_AUTO):
+        cfg = L.bw_server_config(hbm_budget, pinned, lanes, max_groups, num_primes, path)
+        h = ctypes.c_void_p()
+        check(lib.bw_server_create(ctypes.byref(h), ctypes.byref(cfg)))
+        self._h = h
+        self._live = {}
+
+    def prewarm(self, max_log_n, path=L.BW_PATH_AUTO):
+        check(lib.bw_server_prewarm(self._h, path, max_log_n))
+
+    def submit(self, a, b, out=None, path=L.BW_PATH_AUTO):
+        a = _as_u32(a)
+        b = a if b is a else _as_u32(b)
+        if out is None:
+            out = np.zeros(a.size + b.size, dtype=np.uint32)
+        t = ctypes.c_uint64()
+        check(lib.bw_server_submit(self._h, path, _ptr(a), a.size, _ptr(b), b.size, _ptr(out),
+                                   out.size, ctypes.byref(t)))
+        self._live[t.value] = (a, b, out)
+        return t.value
+
+    @staticmethod
+    def _info(i):
+        return {f: getattr(i, f) for f, _ in L.bw_request_info._fields_}
+
+    def wait(self, ticket, timeout_ms=-1):
+        """(out, info) of one request; raises BwError if it failed or, with a
+        timeout, has not finished (it then stays queued)."""
+        info = L.bw_request_info()
+        rc = lib.bw_server_wait(self._h, ticket, timeout_ms, ctypes.byref(info))
+        if rc != L.BW_OK and info.ticket == 0:
+            raise L.BwError(rc, L.last_error())
+        _, _, out = self._live.pop(ticket, (None, None, None))
+        check(rc)
+        return out, self._info(info)
+
+    def harvest(self, max_items=4096):
+        """Finished requests (any order) as info dicts, each with its 'out'."""
+        buf = (L.bw_request_info * max_items)()
+        n = ctypes.c_size_t()
+        check(lib.bw_server_harvest(self._h, buf, max_items, ctypes.byref(n)))
+        res = []
+        for i in range(n.value):
+            d = self._info(buf[i])
+            d["out"] = self._live.pop(d["ticket"], (None, None, None))[2]
+            res.append(d)
+        return res
+
+    def drain(self, timeout_ms=-1):
+        check(lib.bw_server_drain(self._h, timeout_ms))
+
+    def stats(self):
+        st = L.bw_server_stats()
+        check(lib.bw_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in L.bw_server_stats._fields_}
+
+    def close(self):
+        if self._h:
+            lib.bw_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

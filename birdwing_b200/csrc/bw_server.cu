@@ -336,10 +336,12 @@ int launch_group(bw_server* s, Group* g) {
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(g->pin + g->err_off, g->dmem + g->err_off, 16 + g->out_bytes,
                             cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaFreeAsync(g->dmem, st);
+    if (e == cudaSuccess) {
+        e = cudaFreeAsync(g->dmem, st);
+        if (e == cudaSuccess) g->dmem = nullptr;  // released in stream order
+    }
     if (e == cudaSuccess) e = cudaEventRecord(g->ev, st);
     if (e != cudaSuccess) return bw_fail(BW_ECUDA, "launch: %s", cudaGetErrorString(e));
-    g->dmem = nullptr;  // owned by the stream-ordered free now
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->launches += small ? 1 : 4;
@@ -446,10 +448,10 @@ void complete_group(bw_server* s, Group* g) {
             const uint32_t* hw = reinterpret_cast<const uint32_t*>(g->pin);
             for (Req* r : g->reqs) memcpy(r->c, hw + r->off_c, (r->la + r->lb) * 4);
         }
-    } else if (g->dmem) {
-        // launch failed before the stream-ordered free was enqueued
+    } else {
+        // the launch failed part way: let what was enqueued finish
         cudaStreamSynchronize(s->lanes[g->lane]);
-        cudaFree(g->dmem);
+        if (g->dmem) cudaFree(g->dmem);
     }
     const auto t = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
@@ -571,13 +573,22 @@ extern "C" int bw_server_destroy(bw_server* s) {
             s->finished.push_back(r);
         }
         s->cv_done.notify_all();
-        s->cv_done.wait(lk, [&] { return s->in_flight.empty(); });
         s->stop = true;
     }
+    // the engine stops launching; the completer finishes what is in flight
     s->cv_engine.notify_all();
-    s->cv_complete.notify_all();
     if (s->engine.joinable()) s->engine.join();
+    s->cv_complete.notify_all();
     if (s->completer.joinable()) s->completer.join();
+    for (;;) {
+        Group* g = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->in_flight.empty()) break;
+            g = s->in_flight.front();
+        }
+        complete_group(s, g);
+    }
     for (cudaStream_t st : s->lanes) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);

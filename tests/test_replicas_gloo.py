@@ -1,0 +1,88 @@
+"""Multi-process host logic of bench.py on CPU (gloo, world size 2): products
+are independent, so N ranks run N replicas with no collective on the data
+path; the only cross-rank steps are the barrier, the max over ranks of the
+timed region and the sum of counts.  Also: the reference arm prints on rank 0
+only and every other rank exits quietly."""
+import io
+import json
+import os
+import socket
+import sys
+from contextlib import redirect_stdout
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        # rank r's timed region took 10 * (r + 1) ms for 4 * (r + 1) products
+        t_ms, done = bench.reduce_over_ranks([10.0 * (rank + 1), 4.0 * (rank + 1)],
+                                             ["max", "sum"])
+        value = bench.job_throughput(4, world, t_ms)
+        dist.barrier()
+        q.put((rank, t_ms, done, value))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_job_throughput():
+    world, port = 2, free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(world))
+    for rank, t_ms, done, value in res:
+        assert t_ms == 20.0            # the slowest rank
+        assert done == 12.0            # 4 + 8
+        assert value == pytest.approx(2 * 4 / 0.020)
+
+
+def test_single_process_reduction_is_identity():
+    import bench
+    assert bench.reduce_over_ranks([3.5, 2.0], ["max", "sum"]) == [3.5, 2.0]
+    assert bench.job_throughput(10, 1, 5.0) == pytest.approx(2000.0)
+
+
+def test_reference_arm_prints_on_rank_zero_only(monkeypatch):
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    args = bench.parse_args_list(["--impl", "reference", "--config", "1", "--steps", "1",
+                                  "--warmup", "0"])
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.run_reference(args)
+    assert buf.getvalue() == ""
+
+
+def test_reference_arm_line_on_rank_zero(monkeypatch):
+    import bench
+    monkeypatch.setenv("RANK", "0")
+    args = bench.parse_args_list(["--impl", "reference", "--config", "1", "--steps", "1",
+                                  "--warmup", "0"])
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.run_reference(args)
+    line = json.loads(buf.getvalue())
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == "port"
