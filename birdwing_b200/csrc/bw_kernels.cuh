@@ -21,8 +21,9 @@
 // bit-reversed input and natural output.  Stage s (m = 2^s groups) uses the
 // twiddle table entries W[m .. 2m), W[m + i] = w_{2m}^{bitrev_s(i)}.  Each
 // round processes up to 2^RLOG elements per thread in registers (radix 8 or
-// 16); rounds exchange data through swizzled shared memory.  Stage twiddle
-// tables are staged in shared memory when they fit.  The inter-pass twiddle
+// 16); rounds exchange data through swizzled shared memory.  Stage twiddles
+// are read through L1 (the column pass stages them in shared memory when the
+// plan asks for it, BW_PLAN_TW_SMEM).  The inter-pass twiddle
 // of a row is split as w_n^(c k1) = F[c mod 2^a] G[c >> a] with per-row
 // tables F, G (about 2 sqrt(C) entries) built in shared memory at the start
 // of K2, their Shoup companions computed on the device.
