@@ -554,6 +554,8 @@ def run_open_loop(srv, pool, expect, rate, duration, seed):
     def take_finished():
         nonlocal bad, checked, done_in_window
         for d in srv.harvest(8192):
+            if d["ticket"] not in owner:
+                continue
             i, out, chk = owner.pop(d["ticket"])
             if d["status"] != 0:
                 bad += 1

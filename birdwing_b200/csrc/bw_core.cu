@@ -359,10 +359,17 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
                                log_n);
         }
         const int log_cols_outer = pl->log_c + pl->log_r2;  // row length of the outer pass
-        // column tile: 64 KiB of residues per shared-memory buffer
+        // column tile: 64 KiB of residues per shared-memory buffer (128 KiB
+        // with BW_PLAN_WIDE_COLS: wider row segments per CTA, fewer CTAs per SM)
+        const bool wide = (flags & BW_PLAN_WIDE_COLS) != 0;
+        const size_t tile_bytes = wide ? 131072 : 65536;
+        auto fits = [&](int cb) {
+            const size_t elems = (size_t)1 << (pl->log_r + cb);
+            // the forward column pass also stages the tile's 32-bit coefficients
+            return w * elems <= tile_bytes && (!wide || (w + 4) * elems <= 196608);
+        };
         int log_cb = 0;
-        while (log_cb < log_cols_outer && ((size_t)w << (pl->log_r + log_cb + 1)) <= 65536)
-            ++log_cb;
+        while (log_cb < log_cols_outer && fits(log_cb + 1)) ++log_cb;
         pl->log_cb = log_cb;
         if (pl->log_r2) {
             int l2 = 0;

@@ -174,6 +174,7 @@ struct bw_server {
     std::vector<cudaEvent_t> free_events;
     uint64_t next_id = 1;
     size_t bytes_in_flight = 0, peak_bytes = 0, pinned_in_flight = 0;
+    size_t launching = 0;  // requests admitted whose group is not yet in flight
     uint64_t submitted = 0, completed = 0, rejected = 0, failed = 0, groups = 0, launches = 0;
     size_t max_group = 0;
 
@@ -388,6 +389,7 @@ void engine_loop(bw_server* s) {
             continue;
         }
         const auto t_admit = Clock::now();
+        s->launching += take.size();
         s->bytes_in_flight += bytes;
         s->pinned_in_flight += pin;
         s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_flight + plan_b);
@@ -425,6 +427,7 @@ void engine_loop(bw_server* s) {
             s->max_group = std::max(s->max_group, g->reqs.size());
             s->in_flight.push_back(g);
         }
+        s->launching -= take.size();
         s->cv_complete.notify_all();
     }
 }
@@ -711,7 +714,7 @@ extern "C" int bw_server_drain(bw_server* s, int timeout_ms) {
     bw_clear_error();
     if (!s) return bw_fail(BW_EINVAL, "NULL server");
     std::unique_lock<std::mutex> lk(s->mu);
-    auto idle = [&] { return s->pending.empty() && s->in_flight.empty(); };
+    auto idle = [&] { return s->pending.empty() && s->launching == 0 && s->in_flight.empty(); };
     if (timeout_ms < 0) {
         s->cv_done.wait(lk, idle);
     } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), idle)) {

@@ -81,6 +81,9 @@ extern "C" {
 #define BW_PLAN_RADIX8      (1u << 16)
 #define BW_PLAN_TW_SMEM     (1u << 17)
 #define BW_PLAN_THREE_PASS  (1u << 18)
+/* Column-pass tiles of up to 128 KiB of residues instead of 64 KiB (twice
+ * the columns per CTA: longer contiguous row segments, fewer CTAs per SM). */
+#define BW_PLAN_WIDE_COLS   (1u << 19)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
