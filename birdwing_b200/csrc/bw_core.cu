@@ -319,6 +319,15 @@ static int choose_path(size_t la, size_t lb) {
     return BW_PATH_P64;
 }
 
+// Streaming multiprocessors of the current device (148 on a B200).
+static unsigned sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+        return 148;
+    return (unsigned)n;
+}
+
 int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int mode) {
     pl->path = path;
     pl->K = K;
@@ -370,6 +379,11 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         };
         int log_cb = 0;
         while (log_cb < log_cols_outer && fits(log_cb + 1)) ++log_cb;
+        // small transforms: narrower tiles so that the column passes still
+        // put two CTAs on every SM (rows keep >= 16-byte segments)
+        const int min_cb = w == 8 ? 1 : 2;
+        const unsigned sms = sm_count();
+        while (log_cb > min_cb && (2u << (log_cols_outer - log_cb)) < 2u * sms) --log_cb;
         pl->log_cb = log_cb;
         if (pl->log_r2) {
             int l2 = 0;
