@@ -26,6 +26,7 @@ BW_PATH_P64 = 64
 
 BW_PTR_HOST = 0
 BW_PTR_DEVICE = 1
+BW_PTR_HOST_ASYNC = 2
 
 BW_PLAN_RADIX8 = 1 << 16
 BW_PLAN_TW_SMEM = 1 << 17

@@ -163,6 +163,16 @@ class Context:
                             ctypes.byref(t) if timing else None))
         return (out, t.as_dict()) if timing else out
 
+    def multiply_async(self, a, b, out):
+        """Host arrays (pinned for real overlap): enqueue copy-in, product and
+        copy-out and return at once; the arrays must stay alive and unchanged
+        until sync()."""
+        a = _as_u32(a)
+        b = a if b is a else _as_u32(b)
+        check(lib.bw_multiply(self._h, _ptr(a), a.size, _ptr(b), b.size, _ptr(out), out.size,
+                              L.BW_PTR_HOST_ASYNC, None))
+        return out
+
     def multiply_device(self, a_ptr, la, b_ptr, lb, c_ptr, lc, timing=False):
         """Device pointers (ints); enqueues on the context stream."""
         t = L.bw_timing()

@@ -72,6 +72,10 @@ struct Ar32 {
     }
     // forward-transform output range [0, 4p) -> [0, 2p)
     __device__ __forceinline__ T fwd_to_2p(T a) const { return red2(a); }
+    // inverse-transform output range [0, 2p) -> [0, p)
+    __device__ __forceinline__ T inv_out(T a) const { return red1(a); }
+    // x * w for a twiddle applied between transform passes, in [0, 2p)
+    __device__ __forceinline__ T mulc(T x, T w, T wq) const { return shoup(x, w, wq); }
     // Shoup companion floor(w 2^32 / p) of w < p
     __device__ __forceinline__ T companion(T w) const {
         return (uint32_t)((((uint64_t)w) << 32) / p);
@@ -79,11 +83,14 @@ struct Ar32 {
 };
 
 // The 64-bit path's primes are p = c 2^32 + 1 with 2^61 <= p < 2^64 / 6 (62
-// bits).  The forward (CT) transform keeps values in [0, 6p + 2^32): its
-// Shoup quotient omits the x0*v0 partial product (q may be 2 short, so the
-// product lies in [0, 3p)), and its input reduction compares the high word
-// only (subtract 3p when hi > 3c).  The inverse (GS) transform uses the exact
-// quotient and keeps values in [0, 2p).
+// bits).  Every multiplication by a constant inside and between the transforms
+// uses the truncated Shoup quotient, which omits the x0*v0 partial product (q
+// may be 2 short, so the product lies in [0, 3p)).  The forward (CT)
+// transform keeps values in [0, 6p + 2^32); its input reduction compares the
+// high word only (subtract 3p when hi > 3c).  The inverse (GS) transform keeps
+// values in [0, 3p): sums are reduced by one conditional subtraction of 3p,
+// differences are offset by 3p (6p < 2^64).  Garner and the final scalings
+// use the exact quotient.
 struct Ar64 {
     using T = uint64_t;
     static constexpr int BITS = 64;
@@ -188,26 +195,30 @@ struct Ar64 {
         a = x + t;
         b = x - t + p3;
     }
-    // inverse GS butterfly, inputs/outputs in [0, 2p)
+    // inverse GS butterfly, inputs/outputs in [0, 3p)
     __device__ __forceinline__ void gs(T& a, T& b, T w, T wq) const {
-        const T u = a + b;
-        const T v = a - b + p2;
-        a = red2(u);
-        b = shoup(v, w, wq);
+        const T u = a + b;       // [0, 6p)
+        const T v = a - b + p3;  // (0, 6p)
+        a = min(u, u - p3);
+        b = shoup3(v, w, wq);
     }
-    // twiddle-1 butterflies of stage 0 (inputs known to be in [0, 2p))
+    // twiddle-1 butterflies of stage 0 (inputs in [0, 3p))
     __device__ __forceinline__ void ct1(T& a, T& b) const {
         const T x = a;
         a = x + b;
         b = x - b + p3;
     }
     __device__ __forceinline__ void gs1(T& a, T& b) const {
-        const T x = a;
-        a = red2(x + b);
-        b = red2(x - b + p2);
+        const T u = a + b, v = a - b + p3;
+        a = min(u, u - p3);
+        b = min(v, v - p3);
     }
     // forward-transform output range [0, 6p + 2^32) -> [0, 2p)
     __device__ __forceinline__ T fwd_to_2p(T a) const { return red2(min(a, a - p4)); }
+    // inverse-transform output range [0, 3p) -> [0, p)
+    __device__ __forceinline__ T inv_out(T a) const { return red1(min(a, a - p2)); }
+    // x * w for a twiddle applied between transform passes, in [0, 3p)
+    __device__ __forceinline__ T mulc(T x, T w, T wq) const { return shoup3(x, w, wq); }
     // Shoup companion floor(w 2^64 / p) of w < p by a Barrett step with
     // mu = floor(2^128 / p): the estimate is at most 2 short.
     __device__ __forceinline__ T companion(T w) const {

@@ -381,8 +381,9 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         while (log_cb < log_cols_outer && fits(log_cb + 1)) ++log_cb;
         // small transforms: narrower tiles so that the column passes still
         // put two CTAs on every SM (rows keep >= 16-byte segments)
+        // (single products only: a batch group has a grid dimension per product)
         const int min_cb = w == 8 ? 1 : 2;
-        const unsigned sms = sm_count();
+        const unsigned sms = mode == 2 ? sm_count() : 0u;
         while (log_cb > min_cb && (2u << (log_cols_outer - log_cb)) < 2u * sms) --log_cb;
         pl->log_cb = log_cb;
         if (pl->log_r2) {
@@ -429,7 +430,7 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     const size_t half = ((size_t)1 << log_n) / 2;
     pl->zt_a = pl->nca <= half;
     pl->zt_b = pl->ncb <= half;
-    rc = bw_plan_setup(pl, path, K, log_n, flags, 0);
+    rc = bw_plan_setup(pl, path, K, log_n, flags, 2);
     if (rc) {
         delete pl;
         return rc;
@@ -489,7 +490,15 @@ struct bw_ctx {
     uint4* rec_x = nullptr;
     uint32_t* rec_s = nullptr;
     size_t ntiles = 0;
-    uint32_t epoch = 0;
+    // look-back record tag of the last product.  Direct launches use 2, 3, ..;
+    // the replayable graph clears the records and always uses 1.
+    uint32_t epoch = 1;
+    bool capturing = false;
+    cudaGraphExec_t gexec = nullptr;  // device-pointer product, replayed while
+    const void* g_a = nullptr;        // the pointers stay the same
+    const void* g_b = nullptr;
+    const void* g_out = nullptr;
+    bool g_sq = false;
     uint32_t* h_err = nullptr;  // pinned
     cudaEvent_t ev[8] = {};
     int spin_limit = 1 << 22;
@@ -549,6 +558,7 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
 extern "C" int bw_ctx_destroy(bw_ctx* c) {
     if (!c) return BW_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     if (c->h_err) cudaFreeHost(c->h_err);
@@ -741,13 +751,23 @@ int enqueue_carry(bw_ctx* c, uint32_t* out) {
     const size_t n = (size_t)1 << pl->log_n;
     const size_t NL = n / (SPLIT16 ? 2 : 1);
     const size_t M = pl->la + pl->lb;
-    if (++c->epoch >= (1u << 28)) {
-        c->epoch = 1;
-        BW_CUDA(cudaMemsetAsync(c->d_state, 0, c->state_bytes, c->stream));
+    uint32_t epoch = 1;
+    if (!c->capturing) {
+        if (++c->epoch >= (1u << 28)) {
+            c->epoch = 2;
+            BW_CUDA(cudaMemsetAsync(c->d_state + 32, 0, c->state_bytes - 32, c->stream));
+        }
+        epoch = c->epoch;
+    }
+    if (c->ntiles > 1) {
+        const unsigned nb = (unsigned)((c->ntiles - 1 + 255) / 256);
+        k_carry_bounds<Ar, SPLIT16><<<nb, 256, 0, c->stream>>>(
+            pd, reinterpret_cast<const T*>(c->d_res_a), NL, c->rec_x, (uint32_t)c->ntiles,
+            epoch);
     }
     k_garner_carry<Ar, SPLIT16><<<(unsigned)c->ntiles, kCarryThreads, 0, c->stream>>>(
         pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->cst, c->rec_x, c->rec_s,
-        c->epoch, c->inject_wait_fault ? c->epoch + (1u << 27) : c->epoch, c->err,
+        epoch, c->inject_wait_fault ? epoch + (1u << 27) : epoch, c->err,
         c->spin_limit);
     BW_CUDA(cudaGetLastError());
     return BW_OK;
@@ -775,6 +795,49 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 
 }  // namespace
 
+// Device-pointer product through a CUDA graph of the whole pipeline (look-back
+// records cleared, K1..K4), captured on first use and replayed while a, b,
+// out and the squaring choice stay the same.  Returns 1 when a graph cannot
+// be used (the stream is already being captured by the caller).
+static int launch_graph(bw_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t* out, bool sq) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return 1;
+    if (!c->gexec || c->g_a != a || c->g_b != b || c->g_out != out || c->g_sq != sq) {
+        if (c->gexec) {
+            cudaGraphExecDestroy(c->gexec);
+            c->gexec = nullptr;
+        }
+        int rc = bw_set_kernel_attrs();
+        if (rc) return rc;
+        BW_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        cudaError_t e = cudaMemsetAsync(c->d_state + 32, 0, c->state_bytes - 32, c->stream);
+        rc = e == cudaSuccess ? enqueue_product(c, a, b, out, sq, false) : BW_OK;
+        c->capturing = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+        if (rc || e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (rc) return rc;
+            return bw_fail(BW_ECUDA, "graph capture: %s",
+                           cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&c->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            c->gexec = nullptr;
+            return bw_fail(BW_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        c->g_a = a;
+        c->g_b = b;
+        c->g_out = out;
+        c->g_sq = sq;
+    }
+    BW_CUDA(cudaGraphLaunch(c->gexec, c->stream));
+    return BW_OK;
+}
+
 static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
                        uint32_t* out, size_t lc, unsigned flags, bw_timing* tm, bool square) {
     bw_clear_error();
@@ -792,9 +855,15 @@ static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* 
     if (lc < M) return bw_fail(BW_EINVAL, "output has %zu words, needs %zu", lc, M);
     const bool sq = square || (a == b && la == lb);
     const bool timing = tm != nullptr;
+    if ((flags & BW_PTR_HOST_ASYNC) && ((flags & BW_PTR_DEVICE) || timing))
+        return bw_fail(BW_EINVAL, "BW_PTR_HOST_ASYNC takes host pointers and no timing");
     if (timing) cudaEventRecord(c->ev[0], c->stream);
     int rc;
     if (flags & BW_PTR_DEVICE) {
+        if (!timing && !c->inject_wait_fault) {
+            rc = launch_graph(c, a, b, out, sq);
+            if (rc <= 0) return rc;  // 1: fall back to direct launches
+        }
         if (timing) cudaEventRecord(c->ev[1], c->stream);
         rc = enqueue_product(c, a, b, out, sq, timing);
         if (rc) return rc;
@@ -816,6 +885,7 @@ static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* 
         if (timing) cudaEventRecord(c->ev[5], c->stream);
         BW_CUDA(cudaMemcpyAsync(out, c->d_out, M * 4, cudaMemcpyDeviceToHost, c->stream));
         if (timing) cudaEventRecord(c->ev[6], c->stream);
+        if (flags & BW_PTR_HOST_ASYNC) return BW_OK;  // bw_ctx_sync reports errors
         rc = read_device_errors(c);
         if (rc) return rc;
     }

@@ -24,8 +24,10 @@ struct bw_plan {
 };
 
 // Split, tables and constants of a plan for transform length 2^log_n.
-// mode 0: the 4-step pipeline (two or three passes); mode 1: single-pass
-// products of one CTA each (n-point stage tables and the n^-1 scale).
+// mode 0: the 4-step pipeline (two or three passes) for batch groups;
+// mode 1: single-pass products of one CTA each (n-point stage tables and the
+// n^-1 scale); mode 2: the 4-step pipeline for one product at a time, with
+// column tiles narrowed for small n so that the column passes fill the SMs.
 int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int mode);
 
 // Set the dynamic shared-memory limit of every kernel instantiation once.

@@ -454,8 +454,8 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
 
     for (int i = threadIdx.x; i < C; i += NT) {
         const Tw<T> f = F[i & (nf - 1)], g = G[i >> la];
-        bufA[swz<T>(i)] = ar.shoup(ar.shoup(ga[i], f.w, f.wq), g.w, g.wq);
-        if (!square) bufB[swz<T>(i)] = ar.shoup(ar.shoup(gb[i], f.w, f.wq), g.w, g.wq);
+        bufA[swz<T>(i)] = ar.mulc(ar.mulc(ga[i], f.w, f.wq), g.w, g.wq);
+        if (!square) bufB[swz<T>(i)] = ar.mulc(ar.mulc(gb[i], f.w, f.wq), g.w, g.wq);
     }
     __syncthreads();
 
@@ -463,7 +463,7 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     auto ldA = [&](int, int idx) -> T { return bufA[swz<T>(idx)]; };
     auto st_glob = [&](int idx, T v) {
         const Tw<T> f = Fi[idx & (nf - 1)], g = Gi[idx >> la];
-        ga[idx] = ar.shoup(ar.shoup(v, f.w, f.wq), g.w, g.wq);
+        ga[idx] = ar.mulc(ar.mulc(v, f.w, f.wq), g.w, g.wq);
     };
 
     // forward rounds: A fully (all but the last when squaring), B all but the
@@ -608,7 +608,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
         for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x) {
             const int i2 = e >> log_cb, v = e & (CB - 1);
             const Tw<T> a = Tcol[v], b = Trow[i2];
-            buf[swz<T>(e)] = ar.shoup(ar.shoup(g[((size_t)i2 << log_c) + c0 + v], a.w, a.wq),
+            buf[swz<T>(e)] = ar.mulc(ar.mulc(g[((size_t)i2 << log_c) + c0 + v], a.w, a.wq),
                                       b.w, b.wq);
         }
         __syncthreads();
@@ -638,7 +638,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
                 if (last) {
                     const Tw<T> a = Tcol[v], b = Trow[idx];
                     g[((size_t)idx << log_c) + c0 + v] =
-                        ar.shoup(ar.shoup(val, a.w, a.wq), b.w, b.wq);
+                        ar.mulc(ar.mulc(val, a.w, a.wq), b.w, b.wq);
                 } else {
                     buf[swz<T>((idx << log_cb) + v)] = val;
                 }
@@ -688,7 +688,7 @@ __device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::
         };
         auto st = [&](int v, int idx, T val) {
             if (last) {
-                g[(size_t)idx * C + c0 + v] = ar.red1(val);
+                g[(size_t)idx * C + c0 + v] = ar.inv_out(val);
             } else {
                 buf[swz<T>((idx << log_cb) + v)] = val;
             }
@@ -1026,6 +1026,32 @@ __device__ __forceinline__ void garner_carry_body(
         for (int e = 0; e < E; ++e)
             if (j0 + e < M) out[j0 + e] = w[e];
     }
+}
+
+// Carry words of the last thread of every tile but the last (its 8 words'
+// carry-out with carry-in zero), published under `epoch` before K4 runs.
+// K4 tile t then finds tile t-1's record ready and waits only on the 1-bit
+// look-back, not on its predecessor's Garner phase.  One thread per tile.
+template <class Ar, bool SPLIT16>
+__global__ void __launch_bounds__(256)
+k_carry_bounds(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res, size_t NL,
+               uint4* __restrict__ rec_x, uint32_t ntiles, uint32_t epoch) {
+    constexpr int E = kCarryWordsPerThread;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t + 1 >= ntiles) return;
+    const size_t n = (size_t)1 << P.log_n;
+    const size_t j0 = (size_t)(t + 1) * kCarryTileWords - E;
+    unsigned __int128 D[E];
+    uint32_t bad = 0;  // the tile's own pass reports reconstruction errors
+    garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
+    unsigned __int128 acc = 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc = (acc + D[e]) >> 32;
+    uint32_t* rx = reinterpret_cast<uint32_t*>(rec_x + t);
+    st_relaxed(rx + 0, (uint32_t)acc);
+    st_relaxed(rx + 1, (uint32_t)(acc >> 32));
+    st_relaxed(rx + 2, (uint32_t)(acc >> 64));
+    st_release(rx + 3, epoch);
 }
 
 template <class Ar, bool SPLIT16>

@@ -91,6 +91,14 @@ extern "C" {
                                 synchronises                                 */
 #define BW_PTR_DEVICE  1u    /* a, b, c are device pointers: the call only
                                 enqueues work on the context's stream        */
+#define BW_PTR_HOST_ASYNC 2u /* a, b, c are host pointers (pinned, for the
+                                copies to be asynchronous): the call enqueues
+                                copy-in, product and copy-out on the context's
+                                stream and returns; the buffers must stay
+                                valid until bw_ctx_sync, which also reports
+                                device-side errors.  Two contexts used in turn
+                                overlap one product's copies with the other's
+                                kernels.  timing must be NULL.               */
 
 /* Opaque handles.  A plan owns the per-size device tables (twiddles, Garner
  * constants); a context owns device scratch and a stream and borrows its

@@ -311,3 +311,61 @@ def test_config4_plain_huge():
         assert C % m == (A % m) * (B % m) % m, m
     del A, B, C
     assert (got == gmp_ref.mul(a, b)).all()
+
+
+def test_async_host_mode_two_contexts():
+    # BW_PTR_HOST_ASYNC: two contexts of one plan used in turn, pinned buffers
+    import torch
+    rng = np.random.default_rng(31)
+    la, lb = 50000, 30001
+    pairs = [(rand_words(la, rng), rand_words(lb, rng)) for _ in range(6)]
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    ins = [(pinned(a), pinned(b)) for a, b in pairs]
+    outs = [pinned(np.zeros(la + lb, dtype=np.uint32)) for _ in pairs]
+    with bw.Plan(la, lb, 64, 2) as p, bw.Context(p) as c0, bw.Context(p) as c1:
+        ctxs = [c0, c1]
+        for i, ((a, b), o) in enumerate(zip(ins, outs)):
+            c = ctxs[i % 2]
+            if i >= 2:
+                c.sync()
+            c.multiply_async(a, b, o)
+        c0.sync()
+        c1.sync()
+        # timing cannot be asked for in this mode
+        import ctypes
+        t = bw._lib.bw_timing()
+        rc = bw.lib.bw_multiply(c0._h, bw.api._ptr(ins[0][0]), la, bw.api._ptr(ins[0][1]), lb,
+                                bw.api._ptr(outs[0]), la + lb, bw._lib.BW_PTR_HOST_ASYNC,
+                                ctypes.byref(t))
+        assert rc == bw._lib.BW_EINVAL
+    for (a, b), o in zip(pairs, outs):
+        assert (o == gmp_ref.mul(a, b)).all()
+
+
+@pytest.mark.parametrize("path,K,la,lb", [(64, 2, 70000, 50000), (32, 3, 3000, 2999),
+                                          (64, 3, 5000, 1)])
+def test_device_pointer_graph_replay(path, K, la, lb):
+    # device-pointer products replay one captured graph while the pointers
+    # stay the same; new values every time, direct (timed) launches in
+    # between, and a pointer change recaptures
+    import torch
+    rng = np.random.default_rng(41 + la)
+    with bw.Plan(la, lb, path, K) as p, bw.Context(p) as c:
+        da = torch.empty(la, dtype=torch.int32, device="cuda")
+        db = torch.empty(lb, dtype=torch.int32, device="cuda")
+        dc = torch.empty(la + lb, dtype=torch.int32, device="cuda")
+        dc2 = torch.empty(la + lb, dtype=torch.int32, device="cuda")
+        for it in range(5):
+            a, b = rand_words(la, rng), rand_words(lb, rng)
+            da.copy_(torch.from_numpy(a.view(np.int32)))
+            db.copy_(torch.from_numpy(b.view(np.int32)))
+            torch.cuda.synchronize()
+            out = dc2 if it == 3 else dc
+            c.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, out.data_ptr(), la + lb,
+                              timing=(it == 2))
+            c.sync()
+            got = out.cpu().numpy().view(np.uint32)
+            assert (got == gmp_ref.mul(a, b)).all(), it
