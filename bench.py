@@ -62,7 +62,8 @@ BATCH_CONFIGS = {
 SERVE_CONFIGS = {
     "5": (1024, 5, 2,
           "serving: open-loop Poisson arrivals, operands 2^10..2^24 bits log-uniform, 20% "
-          "squarings, second operand 1/8x..1x, 64-bit path, 2 primes, 120 GiB admission budget"),
+          "squarings, second operand 1/8x..1x, prime path chosen per request (automatic), "
+          "2 primes, 120 GiB admission budget"),
 }
 
 

@@ -489,7 +489,7 @@ extern "C" int bw_batch_add(bw_batch* bt, int path, const uint32_t* a, size_t la
     bw_clear_error();
     if (!bt || !a || !b || !c) return bw_fail(BW_EINVAL, "NULL argument");
     if (lc < la + lb) return bw_fail(BW_EINVAL, "output has %zu words, needs %zu", lc, la + lb);
-    if (path == BW_PATH_AUTO) path = BW_PATH_P64;
+    if (path == BW_PATH_AUTO) path = bw_choose_path(bt->K, la, lb);
     int log_n = 0;
     int rc = bw_check_size(path, bt->K, la, lb, &log_n);
     if (rc) return rc;

@@ -530,7 +530,7 @@ extern "C" int bw_server_create(bw_server** out, const bw_server_config* cfg) {
         return bw_fail(BW_EINVAL, "unknown path %d", c.path);
     bw_server* s = new bw_server();
     s->K = c.num_primes ? c.num_primes : 2;
-    s->default_path = c.path == BW_PATH_AUTO ? BW_PATH_P64 : c.path;
+    s->default_path = c.path;  // BW_PATH_AUTO: chosen per request
     s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : (size_t)120 << 30;
     const int nl = c.lanes > 0 ? std::min(c.lanes, 64) : 8;
     s->max_groups = c.max_groups_in_flight > 0 ? c.max_groups_in_flight : 2 * nl;
@@ -611,12 +611,19 @@ extern "C" int bw_server_prewarm(bw_server* s, int path, int max_log_n) {
     bw_clear_error();
     if (!s) return bw_fail(BW_EINVAL, "NULL server");
     if (path == BW_PATH_AUTO) path = s->default_path;
-    if (path != BW_PATH_P32 && path != BW_PATH_P64) return bw_fail(BW_EINVAL, "bad path");
-    max_log_n = std::min(max_log_n, std::min(kMaxGroupLogN, bw_path_max_log_n(path, s->K)));
-    for (int ln = 4; ln <= max_log_n; ++ln) {
-        bw_plan* pl = nullptr;
-        const int rc = get_plan(s, path, ln, &pl);
-        if (rc) return rc;
+    if (path != BW_PATH_AUTO && path != BW_PATH_P32 && path != BW_PATH_P64)
+        return bw_fail(BW_EINVAL, "bad path");
+    // AUTO: the 32-bit path's lengths that automatic choice uses, and the
+    // 64-bit path's up to max_log_n
+    for (const int pth : {BW_PATH_P32, BW_PATH_P64}) {
+        if (path != BW_PATH_AUTO && path != pth) continue;
+        int top = std::min(max_log_n, std::min(kMaxGroupLogN, bw_path_max_log_n(pth, s->K)));
+        if (path == BW_PATH_AUTO && pth == BW_PATH_P32) top = std::min(top, 21);
+        for (int ln = 4; ln <= top; ++ln) {
+            bw_plan* pl = nullptr;
+            const int rc = get_plan(s, pth, ln, &pl);
+            if (rc) return rc;
+        }
     }
     return BW_OK;
 }
@@ -628,6 +635,7 @@ extern "C" int bw_server_submit(bw_server* s, int path, const uint32_t* a, size_
     if (!s || !a || !b || !c || !ticket) return bw_fail(BW_EINVAL, "NULL argument");
     if (lc < la + lb) return bw_fail(BW_EINVAL, "output has %zu words, needs %zu", lc, la + lb);
     if (path == BW_PATH_AUTO) path = s->default_path;
+    if (path == BW_PATH_AUTO) path = bw_choose_path(s->K, la, lb);
     int log_n = 0;
     int rc = bw_check_size(path, s->K, la, lb, &log_n);
     if (rc) return rc;

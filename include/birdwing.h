@@ -160,8 +160,9 @@ int bw_size_supported(int path, int num_primes, size_t la, size_t lb);
 
 /* Build the plan (twiddle tables on the device, Garner constants) for
  * products of la x lb u32 words.  path = BW_PATH_AUTO picks the faster path
- * for the size; num_primes = 0 picks the smallest K whose product bound
- * holds (2 for both paths).  The plan is bound to the current CUDA device. */
+ * for the size: the 32-bit path while its transform has at most 2^21 points
+ * (operands up to about 2^24 bits), the 64-bit path beyond; num_primes = 0
+ * picks K = 2.  The plan is bound to the current CUDA device. */
 int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb,
                    int num_primes, unsigned flags);
 int bw_plan_destroy(bw_plan* plan);
@@ -280,7 +281,8 @@ int bw_batch_destroy(bw_batch* batch);
 int bw_batch_clear(bw_batch* batch);
 /* Append c[0 .. la+lb) = a * b (host pointers, read at every run with
  * BW_BATCH_UPLOAD; c written at every run with BW_BATCH_DOWNLOAD).
- * a == b with la == lb squares.  path BW_PATH_AUTO means P64. */
+ * a == b with la == lb squares.  path BW_PATH_AUTO chooses as
+ * bw_plan_create does. */
 int bw_batch_add(bw_batch* batch, int path, const uint32_t* a, size_t la,
                  const uint32_t* b, size_t lb, uint32_t* c, size_t lc);
 /* Run the batch (blocking).  The first run after bw_batch_add/clear builds
@@ -322,7 +324,8 @@ typedef struct bw_server_config {
     int      lanes;                 /* streams groups are issued on (0 = 8) */
     int      max_groups_in_flight;  /* (0 = 2 * lanes)                      */
     int      num_primes;            /* K (0 = 2)                            */
-    int      path;                  /* default path (BW_PATH_AUTO = P64)    */
+    int      path;                  /* default path (BW_PATH_AUTO: chosen
+                                       per request, as for bw_plan_create)  */
 } bw_server_config;
 
 /* One finished request.  Times are microseconds on a steady clock since the
