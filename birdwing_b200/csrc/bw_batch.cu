@@ -60,7 +60,12 @@ struct TuneVal {
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 
+// The one-CTA kernel holds both operands' transforms in shared memory: up to
+// 2^13 (64-bit) or 2^14 (32-bit) points.  By default it runs up to 2^12
+// points; beyond that the 4-step kernels measured faster on both paths (the
+// one-CTA kernel's shared memory then holds one or two CTAs per SM).
 int small_max_log(int path) { return path == BW_PATH_P64 ? 13 : 14; }
+constexpr int kSmallDefaultLog = 12;
 
 // Products per bucket: kb_fwd_col puts 2 * products in gridDim.z (<= 65535).
 constexpr size_t kMaxBucket = 16384;
@@ -69,7 +74,7 @@ TuneVal tune_get(int path, int K, int log_n) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(TuneKey{path, K, log_n});
     if (it != g_tune.end()) return it->second;
-    return TuneVal{log_n <= small_max_log(path) ? 1 : 0, 0, 0.f};
+    return TuneVal{log_n <= kSmallDefaultLog ? 1 : 0, 0, 0.f};
 }
 
 struct Prod {
@@ -586,9 +591,10 @@ extern "C" int bw_batch_autotune(bw_batch* bt, int reps) {
         if (cands.count(key)) continue;
         std::vector<TuneVal> v;
         if (p.log_n <= small_max_log(p.path)) v.push_back(TuneVal{1, 0, 0.f});
-        const int c0 = (p.log_n + 1) / 2;
-        for (int lc : {c0 - 1, c0, c0 + 1})
-            if (lc >= 2 && lc <= p.log_n - 2 && p.log_n - lc <= 13) v.push_back(TuneVal{0, lc, 0.f});
+        // 4-step splits from square to long rows (columns of 2^2 at least)
+        const int max_c = p.path == BW_PATH_P64 ? 13 : 14;
+        for (int lc = (p.log_n + 1) / 2 - 1; lc <= std::min(max_c, p.log_n - 2); ++lc)
+            if (lc >= 2 && p.log_n - lc <= 13) v.push_back(TuneVal{0, lc, 0.f});
         cands[key] = v;
     }
     // one sub-batch per key with the batch's products of that key

@@ -353,7 +353,12 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         const bool three = (flags & BW_PLAN_THREE_PASS) || log_n > 26;
         const int want_c = (int)((flags >> 8) & 0x1f);
         if (!three) {
-            pl->log_c = std::min(max_c, (log_n + 1) / 2);
+            // one product: a square split; a batch group (mode 0): long rows
+            // (C = 2^min(12, log n - 3) on the 64-bit path) and short columns:
+            // the rows keep every thread of the row pass busy even for small
+            // n, and the group's grid has a product dimension to fill the SMs
+            pl->log_c = mode == 0 ? std::max(std::min(max_c - 1, log_n - 3), (log_n + 1) / 2)
+                                  : std::min(max_c, (log_n + 1) / 2);
             if (want_c) {
                 if (want_c > max_c || want_c >= log_n || log_n - want_c > 13)
                     return bw_fail(BW_EINVAL, "BW_PLAN_LOG_COLS(%d) invalid for n = 2^%d",

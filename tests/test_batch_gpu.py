@@ -25,6 +25,11 @@ def log_n_of(path, la, lb):
     return max(4, (m - 1).bit_length())
 
 
+def default_small(ln):
+    """The library's default kernel form: one CTA per product up to 2^12 points."""
+    return ln <= 12
+
+
 def run_batch(items, K=2):
     """items: [(path, a, b)]; returns outputs in order."""
     with bw.Batch(num_primes=K) as bt:
@@ -79,7 +84,7 @@ def test_power_of_two_product_length(path, small):
     finally:
         for p, a, b in items:
             ln = log_n_of(p, len(a), len(b))
-            bw.set_tune_entry(p, 2, ln, ln <= (13 if p == 64 else 14))
+            bw.set_tune_entry(p, 2, ln, default_small(ln))
     for (p, a, b), got in zip(items, outs):
         assert (got == gmp_ref.mul(a, b)).all(), (p, len(a), len(b))
 
@@ -97,7 +102,7 @@ def test_forms_agree_on_the_same_products(small):
         outs, info = run_batch(items)
     finally:
         for p, ln in keys:
-            bw.set_tune_entry(p, 2, ln, True)
+            bw.set_tune_entry(p, 2, ln, default_small(ln))
     assert info["small_buckets"] == (len(keys) if small else 0)
     for (p, a, b), got in zip(items, outs):
         assert (got == gmp_ref.mul(a, b)).all()
@@ -188,7 +193,7 @@ def test_autotune_and_tune_table_roundtrip():
     bw.load_tune_table(table)
     # restore defaults for the other tests
     for p, ln in keys:
-        bw.set_tune_entry(p, 2, ln, ln <= (13 if p == 64 else 14))
+        bw.set_tune_entry(p, 2, ln, default_small(ln))
 
 
 def test_uneven_mix_vs_gmp():
