@@ -296,7 +296,7 @@ def batch_model_bytes(items, K, small_max=None):
     """Algorithmic HBM bytes of a batch: per product the plain path's model
     (12*K*n*w + in + out) for 4-step products, and in + out + 2*K*n*w (one
     residue write and read) for products run one CTA each."""
-    small_max = small_max or {64: 13, 32: 14}
+    small_max = small_max or {64: 12, 32: 12}   # the library's default forms
     total = 0
     for p, a, b in items:
         cpw = 2 if p == 32 else 1
