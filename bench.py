@@ -8,7 +8,13 @@ the HBM roofline of the dominant kernel and the product-level algorithmic
 byte model (12*K*n*w + in + out) beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config 1|2|2sq]
+                  [--config 1|2|2sq|4|3|5]
+
+Configurations: 2 (default), 2sq (squaring), 1 (2^20-bit, 32-bit path), 4
+(2^33-bit, n = 2^29, three passes), 3 (4096 batched products of uneven
+sizes, against the plain path looped per product), 5 (serving: open-loop
+Poisson arrivals, p50/p99 latency); prof and 3prof are smaller cases of the
+same kernels for ncu captures.
 
 Multi-GPU: products are independent, so N ranks run N replicas (no
 collective on the data path, "scaling": "weak"); the timed region is
@@ -43,6 +49,9 @@ CONFIGS = {
             "squaring 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
     "1": (1 << 15, 1 << 15, 32, 3, False,
           "plain 2^20-bit x 2^20-bit, 16-bit coefficients, n=2^17, 3 x 30-bit primes"),
+    "4": (1 << 28, 1 << 28, 64, 3, False,
+          "plain huge 2^33-bit x 2^33-bit (1 GiB each), 32-bit coefficients, n=2^29, "
+          "3 x 62-bit primes, three-pass schedule"),
     # a smaller product of the same kernels for ncu captures (working set > L2)
     "prof": (1 << 21, 1 << 21, 64, 2, False,
              "plain 2^26-bit x 2^26-bit, 32-bit coefficients, n=2^22, 2 x 62-bit primes"),
@@ -212,12 +221,35 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def residue_check(a, b, got, count=3, seed=61):
+    """Product check without a full multiprecision multiply: the result's
+    residues mod 2^64 and mod `count` random 61-bit probable primes."""
+    def as_int(w):
+        return int.from_bytes(np.ascontiguousarray(w).view(np.uint8).tobytes(), "little")
+    A, B, C = as_int(a), as_int(b), as_int(got)
+    rng = np.random.default_rng(seed)
+    mods = [1 << 64]
+    while len(mods) < count + 1:
+        m = int(rng.integers(1 << 60, 1 << 61)) | 1
+        if pow(3, m - 1, m) == 1:
+            mods.append(m)
+    return all(C % m == (A % m) * (B % m) % m for m in mods)
+
+
+# configurations too large for a full CPU product inside the baseline budget:
+# the oracle runs a smaller product of the same path and primes, and its time
+# is scaled by n log n (the transforms dominate)
+CPU_SAMPLE_WORDS = {"4": 1 << 22}
+
+
 def cpu_baseline(cfg, budget_s=20.0):
     """The oracle (CPU restatement of the reference's algorithm) with all host
     threads on the same operands: full products until the budget is spent
     (at least one).  GMP mpz_mul (single thread) is reported beside it."""
     from oracle import gmp_ref, oracle
     la, lb, path, K, square, _ = CONFIGS[cfg]
+    if cfg in CPU_SAMPLE_WORDS:
+        return cpu_baseline_scaled(cfg, CPU_SAMPLE_WORDS[cfg], budget_s)
     a, b = operands(cfg, 0)
     cores = os.cpu_count() or 1
     oracle.lib.oracle_set_threads(cores)
@@ -236,6 +268,33 @@ def cpu_baseline(cfg, budget_s=20.0):
                     "impl": f"GMP {gmp_ref.version} mpz_mul, single thread"}}
 
 
+def cpu_baseline_scaled(cfg, words, budget_s):
+    from oracle import gmp_ref, mt64, oracle
+    la, lb, path, K, square, _ = CONFIGS[cfg]
+    a = mt64.random_words_top_fast(words, 1234)
+    b = a if square else mt64.random_words_top_fast(words, 5678)
+    cores = os.cpu_count() or 1
+    oracle.lib.oracle_set_threads(cores)
+    n_done, t0 = 0, time.perf_counter()
+    while True:
+        oracle.multiply(a, b, path, K)
+        n_done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = (time.perf_counter() - t0) / n_done
+    log_s = max(4, (2 * words - 2).bit_length())
+    log_f = max(4, (la + lb - 2).bit_length())
+    scale = ((1 << log_f) * log_f) / ((1 << log_s) * log_s)
+    g = gmp_ref.time_mul(a, b, 1) * scale
+    return {"value": 1.0 / (dt * scale), "unit": "products/s", "cores": cores, "kind": "port",
+            "sample": f"{n_done} product(s) of {words} x {words} words (n = 2^{log_s}) with the "
+                      f"workload's path and primes, oracle/bw_oracle.c on {cores} threads, "
+                      f"{dt:.2f} s each, scaled by n log n to n = 2^{log_f} (x{scale:.1f})",
+            "gmp": {"value": 1.0 / g, "unit": "products/s", "cores": 1,
+                    "impl": f"GMP {gmp_ref.version} mpz_mul, single thread, same sample "
+                            f"and scaling"}}
+
+
 def run_reference(args):
     """--impl reference: the oracle port on the host cores, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -243,6 +302,20 @@ def run_reference(args):
         return
     from oracle import oracle
     la, lb, path, K, square, desc = CONFIGS[args.config]
+    if args.config in CPU_SAMPLE_WORDS:
+        cb = cpu_baseline_scaled(args.config, CPU_SAMPLE_WORDS[args.config], 60.0)
+        v = cb["value"]
+        print(json.dumps({
+            "impl": "reference", "metric": "products/s", "value": v, "unit": "products/s",
+            "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic", "config": {"workload": f"config {args.config}: {desc}",
+                                            "words_a": la, "words_b": lb, "path": path,
+                                            "num_primes": K},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
     a, b = operands(args.config, 0)
     cores = os.cpu_count() or 1
     oracle.lib.oracle_set_threads(cores)
@@ -824,12 +897,20 @@ def main():
         step(False)
     ctx.sync()
     # correctness of the benchmarked product (once, outside the timed region)
+    check = "GMP mpz_mul"
     if rank == 0:
-        from oracle import gmp_ref
         got = dc.cpu().numpy().view(np.uint32)
-        ok = bool((got == gmp_ref.mul(a, b)).all())
+        if args.config in CPU_SAMPLE_WORDS:
+            check = "residues mod 2^64 and three random 61-bit primes"
+            ok = residue_check(a, b, got)
+        else:
+            from oracle import gmp_ref
+            ok = bool((got == gmp_ref.mul(a, b)).all())
+        del got
     else:
         ok = True
+    device_bytes = (plan.info["plan_device_bytes"] + plan.info["ctx_device_bytes"] +
+                    4 * (la + (0 if square else lb)) + 4 * (la + lb))
 
     sampler = ClockSampler(local)
     stage = {k: [] for k in ("fwd_ms", "mul_ms", "intt_ms", "crt_carry_ms")}
@@ -883,9 +964,10 @@ def main():
     # pipelined: two contexts used in turn (BW_PTR_HOST_ASYNC), so one
     # product's copies overlap the other's kernels; every product still
     # copies its operands in and its result out
-    # three in flight: one copying in, one computing, one copying out
+    # three in flight: one copying in, one computing, one copying out (two for
+    # products whose contexts take tens of GiB)
     ring = [(ctx, hc)]
-    for _ in range(2):
+    for _ in range(2 if n < (1 << 27) else 1):
         ring.append((bw.Context(plan),
                      torch.empty(la + lb, dtype=torch.int32).pin_memory().numpy().view(np.uint32)))
     for c_, o_ in ring:
@@ -905,9 +987,12 @@ def main():
     e2e_pipe_total = reduce_over_ranks([1000 * (time.perf_counter() - t0)], ["max"])[0]
     ok_e2e = True
     if rank == 0:
-        from oracle import gmp_ref
-        want = gmp_ref.mul(a, b)
-        ok_e2e = all(bool((o_ == want).all()) for _, o_ in ring)
+        if args.config in CPU_SAMPLE_WORDS:
+            ok_e2e = all(residue_check(a, b, o_) for _, o_ in ring)
+        else:
+            from oracle import gmp_ref
+            want = gmp_ref.mul(a, b)
+            ok_e2e = all(bool((o_ == want).all()) for _, o_ in ring)
     for c_, _ in ring[1:]:
         c_.close()
 
@@ -932,6 +1017,8 @@ def main():
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "correct_vs_gmp": ok,
+            "correctness_check": check,
+            "hbm_footprint_bytes": device_bytes,
             "stage_ms": means,
             "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
