@@ -1,6 +1,6 @@
 """Benchmark of the big-integer multiply path (one JSON line on rank 0).
 
-Workload: BASELINE configuration 2 -- one plain 2^28-bit x 2^28-bit product
+Default workload (configuration 2): one plain 2^28-bit x 2^28-bit product
 (2^23 u32 words each, uniform random with the top bit set, seeded), 32-bit
 coefficients, n = 2^24, two 62-bit primes (64-bit prime path).  A "step" is
 one full product.  Metric: products/s (whole job), with the per-stage times,

@@ -2,7 +2,7 @@
 
 Bit-exact everywhere: this is integer arithmetic.  Small and medium sizes
 are checked against the oracle (the CPU restatement of the reference's
-algorithm) and GMP; the BASELINE sizes against GMP and through
+algorithm) and GMP; the benchmark sizes against GMP and through
 size-independent properties (squaring == self-product, linearity in one
 operand, products mod small primes)."""
 import os
@@ -229,7 +229,7 @@ def test_lookback_wait_fault_is_reported_and_recoverable():
 
 
 def test_config1_plain_small():
-    # 2^20-bit operands (2^15 words), 16-bit
+    # the 2^20-bit workload: 2^20-bit operands (2^15 words), 16-bit
     # coefficients, n = 2^17, three 30-bit primes
     a = mt64.random_words_top(1 << 15, 1234)
     b = mt64.random_words_top(1 << 15, 5678)
@@ -239,7 +239,7 @@ def test_config1_plain_small():
 
 
 def test_config2_plain_large():
-    # 2^28-bit operands (2^23 words), 32-bit
+    # the 2^28-bit workload: 2^28-bit operands (2^23 words), 32-bit
     # coefficients, n = 2^24, 62-bit primes; plus the squaring variant
     a = mt64.random_words_top_fast(1 << 23, 1234)
     b = mt64.random_words_top_fast(1 << 23, 5678)
@@ -291,7 +291,7 @@ def test_three_pass_schedule_vs_gmp_medium():
 
 
 def test_config4_plain_huge():
-    # 2^33-bit operands (2^28 words, 1 GiB each),
+    # the 2^33-bit workload: 2^33-bit operands (2^28 words, 1 GiB each),
     # 32-bit coefficients, n = 2^29, three 62-bit primes, three-pass
     # schedule.  Checked by residues mod 2^64 and mod three random 61-bit
     # primes, and bit-exact against GMP mpz_mul on the host.
