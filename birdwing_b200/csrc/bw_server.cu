@@ -55,6 +55,19 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr size_t kAlign = 256;
+// Operands and results at least this large move by DMA straight between the
+// caller's pinned buffers and the device; smaller ones are staged, where one
+// memcpy beats one more copy call.
+constexpr size_t kDirectBytes = 64 * 1024;
+
+bool is_pinned_host(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();  // pageable memory may report an error: not pinned
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct Req {
@@ -70,8 +83,11 @@ struct Req {
     Clock::time_point t_submit, t_admit, t_launch, t_done;
     int status = 1;         // 1 = not finished
     size_t group_size = 0;
-    // offsets inside the group block (words)
-    size_t off_a = 0, off_b = 0, off_c = 0;
+    // the caller's buffers are pinned host memory (direct DMA when large)
+    bool a_pin = false, b_pin = false, c_pin = false, c_direct = false;
+    // offsets inside the group's device block (words); off_c_pin: the
+    // result's offset in the pinned staging block when it is staged
+    size_t off_a = 0, off_b = 0, off_c = 0, off_c_pin = 0;
 };
 
 // Pinned host blocks by power-of-two size class, cached for reuse; the
@@ -140,7 +156,7 @@ struct Group {
     unsigned char* pin = nullptr;
     size_t pin_cls = 0;
     size_t dev_bytes = 0;
-    size_t err_off = 0, out_off = 0, out_bytes = 0;
+    size_t err_off = 0, err_pin = 0, out_bytes = 0;
     cudaEvent_t ev = nullptr;
     int launch_status = BW_OK;
 };
@@ -258,26 +274,57 @@ int launch_group(bw_server* s, Group* g) {
     size_t max_words = 0;
     for (const Req* r : g->reqs) max_words = std::max(max_words, r->la + r->lb);
     const size_t ntiles = bw_group_ntiles(path, log_n, max_words);
-    // block layout: [desc | inputs | err | outputs | states | res_a | res_b]
+    // Device block: [desc | staged inputs | direct inputs | err | staged
+    // outputs | direct outputs | states | res_a | res_b].  The pinned staging
+    // block holds [desc | staged inputs] and [err | staged outputs], so one
+    // H2D and one D2H copy move every staged operand and result; operands and
+    // results in the caller's own pinned memory (large ones) move by DMA
+    // straight from and to it.
+    auto direct = [](bool pinned, size_t words) { return pinned && words * 4 >= kDirectBytes; };
     size_t off = align_up(np * sizeof(BatchProd), 16);
     for (Req* r : g->reqs) {
-        r->off_a = off / 4;
-        off += 4 * align_up(r->la, 4);
-        if (!r->square) {
+        if (!direct(r->a_pin, r->la)) {
+            r->off_a = off / 4;
+            off += 4 * align_up(r->la, 4);
+        }
+        if (!r->square && !direct(r->b_pin, r->lb)) {
             r->off_b = off / 4;
             off += 4 * align_up(r->lb, 4);
-        } else {
-            r->off_b = r->off_a;
         }
+    }
+    const size_t staged_in_end = off;
+    for (Req* r : g->reqs) {
+        if (direct(r->a_pin, r->la)) {
+            r->off_a = off / 4;
+            off += 4 * align_up(r->la, 4);
+        }
+        if (!r->square && direct(r->b_pin, r->lb)) {
+            r->off_b = off / 4;
+            off += 4 * align_up(r->lb, 4);
+        }
+        if (r->square) r->off_b = r->off_a;
     }
     g->err_off = off;
     off += 16;
-    g->out_off = off;
+    size_t pin_off = staged_in_end;  // err + staged outputs follow the inputs
+    g->err_pin = pin_off;
+    pin_off += 16;
     for (Req* r : g->reqs) {
-        r->off_c = off / 4;
-        off += 4 * align_up(r->la + r->lb, 4);
+        if (!direct(r->c_pin, r->la + r->lb)) {
+            r->off_c = off / 4;
+            r->off_c_pin = pin_off / 4;
+            off += 4 * align_up(r->la + r->lb, 4);
+            pin_off += 4 * align_up(r->la + r->lb, 4);
+        }
     }
-    g->out_bytes = off - g->out_off;
+    g->out_bytes = off - g->err_off - 16;  // staged outputs only
+    for (Req* r : g->reqs) {
+        if (direct(r->c_pin, r->la + r->lb)) {
+            r->off_c = off / 4;
+            r->c_direct = true;
+            off += 4 * align_up(r->la + r->lb, 4);
+        }
+    }
     const size_t st_stride = small ? 0 : bw_group_state_stride(ntiles);
     const size_t st_off = align_up(off, 16);
     off = align_up(st_off + np * st_stride, kAlign);
@@ -287,7 +334,7 @@ int launch_group(bw_server* s, Group* g) {
     const size_t rb_off = off;
     if (!small) off += np * per;
     g->dev_bytes = off;
-    const size_t pin_need = g->out_off + g->out_bytes;
+    const size_t pin_need = pin_off;
 
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -297,14 +344,14 @@ int launch_group(bw_server* s, Group* g) {
     cudaStream_t st = s->lanes[g->lane];
     cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&g->dmem), g->dev_bytes, st);
     if (e != cudaSuccess) return bw_fail(BW_ENOMEM, "cudaMallocAsync: %s", cudaGetErrorString(e));
-    // descriptors and operands into pinned staging
+    // descriptors and staged operands into pinned staging
     BatchProd* desc = reinterpret_cast<BatchProd*>(g->pin);
     uint32_t* hw = reinterpret_cast<uint32_t*>(g->pin);
     uint32_t* dw = reinterpret_cast<uint32_t*>(g->dmem);
     for (size_t q = 0; q < np; ++q) {
         Req* r = g->reqs[q];
-        memcpy(hw + r->off_a, r->a, r->la * 4);
-        if (!r->square) memcpy(hw + r->off_b, r->b, r->lb * 4);
+        if (!direct(r->a_pin, r->la)) memcpy(hw + r->off_a, r->a, r->la * 4);
+        if (!r->square && !direct(r->b_pin, r->lb)) memcpy(hw + r->off_b, r->b, r->lb * 4);
         BatchProd d{};
         d.a = dw + r->off_a;
         d.b = dw + r->off_b;
@@ -318,7 +365,13 @@ int launch_group(bw_server* s, Group* g) {
     }
     const auto t_launch = Clock::now();
     for (Req* r : g->reqs) r->t_launch = t_launch;
-    e = cudaMemcpyAsync(g->dmem, g->pin, g->err_off, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(g->dmem, g->pin, staged_in_end, cudaMemcpyHostToDevice, st);
+    for (Req* r : g->reqs) {
+        if (e == cudaSuccess && direct(r->a_pin, r->la))
+            e = cudaMemcpyAsync(dw + r->off_a, r->a, r->la * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && !r->square && direct(r->b_pin, r->lb))
+            e = cudaMemcpyAsync(dw + r->off_b, r->b, r->lb * 4, cudaMemcpyHostToDevice, st);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(g->dmem + g->err_off, 0, 16, st);
     if (e == cudaSuccess && !small)
         e = cudaMemsetAsync(g->dmem + st_off, 0, np * st_stride, st);
@@ -335,8 +388,12 @@ int launch_group(bw_server* s, Group* g) {
     if (rc) return rc;
     e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(g->pin + g->err_off, g->dmem + g->err_off, 16 + g->out_bytes,
+        e = cudaMemcpyAsync(g->pin + g->err_pin, g->dmem + g->err_off, 16 + g->out_bytes,
                             cudaMemcpyDeviceToHost, st);
+    for (Req* r : g->reqs)
+        if (e == cudaSuccess && r->c_direct)
+            e = cudaMemcpyAsync(r->c, dw + r->off_c, (r->la + r->lb) * 4, cudaMemcpyDeviceToHost,
+                                st);
     if (e == cudaSuccess) {
         e = cudaFreeAsync(g->dmem, st);
         if (e == cudaSuccess) g->dmem = nullptr;  // released in stream order
@@ -440,7 +497,7 @@ void complete_group(bw_server* s, Group* g) {
             status = BW_ECUDA;
         } else {
             uint32_t err = 0;
-            memcpy(&err, g->pin + g->err_off, 4);
+            memcpy(&err, g->pin + g->err_pin, 4);
             if (err & 1u) {
                 status = BW_ETIMEOUT;
             } else if (err) {
@@ -449,7 +506,8 @@ void complete_group(bw_server* s, Group* g) {
         }
         if (status == BW_OK) {
             const uint32_t* hw = reinterpret_cast<const uint32_t*>(g->pin);
-            for (Req* r : g->reqs) memcpy(r->c, hw + r->off_c, (r->la + r->lb) * 4);
+            for (Req* r : g->reqs)
+                if (!r->c_direct) memcpy(r->c, hw + r->off_c_pin, (r->la + r->lb) * 4);
         }
     } else {
         // the launch failed part way: let what was enqueued finish
@@ -650,6 +708,9 @@ extern "C" int bw_server_submit(bw_server* s, int path, const uint32_t* a, size_
     r->la = la;
     r->lb = lb;
     r->square = (a == b && la == lb);
+    r->a_pin = is_pinned_host(a);
+    r->b_pin = r->square ? r->a_pin : is_pinned_host(b);
+    r->c_pin = is_pinned_host(c);
     r->dev_bytes = request_bytes(path, s->K, log_n, la, lb, r->square);
     // staging charge: a group's pinned block is its bytes rounded up to a
     // power of two (at least 4 KiB), so twice the request's own bytes covers

@@ -132,3 +132,35 @@ def test_wait_poll_and_errors():
             srv.wait(t, timeout_ms=0)          # released already
         with pytest.raises(bw.BwError):
             srv.submit(a, a, out=np.zeros(10, dtype=np.uint32))
+
+
+def test_pinned_buffers_move_by_dma():
+    # operands and results in pinned host memory (large ones move by DMA
+    # straight to and from the device), mixed with pageable ones in the same
+    # groups; squarings included
+    import torch
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    rng = np.random.default_rng(9)
+    reqs = []
+    for i, (la, lb) in enumerate([(20000, 17000), (40000, 40000), (3000, 200), (70000, 9000),
+                                  (16384, 16384), (50000, 1), (100, 100), (33000, 33000)]):
+        a = rand_words(la, rng)
+        b = a if i % 4 == 1 else rand_words(lb, rng)
+        if i % 2 == 0:
+            a = pinned(a)
+            b = a if i % 4 == 1 else pinned(b)
+        out = np.zeros(len(a) + len(b), dtype=np.uint32)
+        if i % 3 != 2:
+            out = pinned(out)
+        reqs.append((a, b, out))
+    with bw.Server() as srv:
+        for rep in range(2):
+            tickets = [srv.submit(a, b, out=o) for a, b, o in reqs]   # together: batched
+            for t in tickets:
+                srv.wait(t)
+            for a, b, o in reqs:
+                assert (o == gmp_ref.mul(a, b)).all(), (rep, len(a), len(b))
+                o[:] = 0
