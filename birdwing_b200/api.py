@@ -382,6 +382,23 @@ class Server:
             res.append(d)
         return res
 
+    def harvest_arrays(self, max_items=8192):
+        """Finished requests as numpy columns (ticket, status, submit_us,
+        admit_us, launch_us, done_us, group_size) plus their output arrays,
+        for clients that handle many results per call."""
+        buf = (L.bw_request_info * max_items)()
+        n = ctypes.c_size_t()
+        check(lib.bw_server_harvest(self._h, buf, max_items, ctypes.byref(n)))
+        dt = np.dtype({"names": [f for f, _ in L.bw_request_info._fields_],
+                       "formats": ["<u8", "<i4", "<f8", "<f8", "<f8", "<f8", "<u8", "<u8",
+                                   "<u8", "<u8"],
+                       "offsets": [getattr(L.bw_request_info, f).offset
+                                   for f, _ in L.bw_request_info._fields_],
+                       "itemsize": ctypes.sizeof(L.bw_request_info)})
+        rec = np.frombuffer(buf, dtype=dt, count=n.value).copy()
+        outs = [self._live.pop(int(t), (None, None, None))[2] for t in rec["ticket"]]
+        return rec, outs
+
     def drain(self, timeout_ms=-1):
         check(lib.bw_server_drain(self._h, timeout_ms))
 

@@ -132,6 +132,16 @@ def test_wait_poll_and_errors():
             srv.wait(t, timeout_ms=0)          # released already
         with pytest.raises(bw.BwError):
             srv.submit(a, a, out=np.zeros(10, dtype=np.uint32))
+        # many results per call as numpy columns
+        ops = [(rand_words(n, rng), rand_words(n // 3 + 1, rng)) for n in (10, 5000, 40000)]
+        tickets = [srv.submit(x, y) for x, y in ops]
+        srv.drain()
+        rec, outs = srv.harvest_arrays()
+        assert sorted(rec["ticket"].tolist()) == sorted(tickets)
+        assert (rec["status"] == 0).all() and (rec["done_us"] >= rec["submit_us"]).all()
+        by_ticket = dict(zip(rec["ticket"].tolist(), outs))
+        for t, (x, y) in zip(tickets, ops):
+            assert (by_ticket[t] == gmp_ref.mul(x, y)).all()
 
 
 def test_pinned_buffers_move_by_dma():
