@@ -95,7 +95,7 @@ def parse_args_list(argv):
                     help="batched/serving configurations: skip the plain per-product path")
     ap.add_argument("--duration", type=float, default=10.0,
                     help="serving: seconds of arrivals per swept rate")
-    ap.add_argument("--rate-fracs", default="0.3,0.6,0.85",
+    ap.add_argument("--rate-fracs", default="0.3,0.45,0.6,0.75",
                     help="serving: arrival rates as fractions of the closed-loop capacity")
     ap.add_argument("--log-cols", type=int, default=0,
                     help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")

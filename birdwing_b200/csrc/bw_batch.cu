@@ -186,9 +186,10 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
         return;
     }
     const int R = 1 << pl.log_r, C = 1 << pl.log_c, CB = 1 << pl.log_cb;
-    const size_t smem1 = (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
-    kb_fwd_col<Ar, SPLIT16, 4><<<dim3(C / CB, 1, 2 * np), kColThreads, smem1, s>>>(P, g.d_desc,
-                                                                                  ra, rb);
+    const int CB1 = 1 << pl.log_cb1;
+    const size_t smem1 = (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : 4));
+    kb_fwd_col<Ar, SPLIT16, 4><<<dim3(C / CB1, 1, 2 * np), kColThreads, smem1, s>>>(
+        P, g.d_desc, ra, rb);
     const int la = pl.log_c / 2;
     const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
     const size_t smem2 = ntab * sizeof(Tw<T>) + (size_t)C * sizeof(T) * 2;

@@ -91,11 +91,13 @@ uint32_t bitrev_h(uint32_t x, int bits) {
 // P64: c * 2^32 + 1, the largest such primes below 2^64 / 6 (62 bits,
 //      v2(p-1) = 32; the bound is what the forward butterfly's lazy range
 //      [0, 6p + 2^32) needs).
-// P32: 30-bit primes with v2(p-1) = 24, 26, 25.
+// P32: primes below 2^30 with v2(p-1) = 26, 25, 24: the first two (K = 2)
+//      allow transforms of 2^25 points, and their product (2^56.1) bounds
+//      every product of that length (min(L_A, L_B) (2^16 - 1)^2 < p0 p1).
 const uint64_t kP64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
 const uint64_t kG64[3] = {10, 7, 3};
-const uint64_t kP32[3] = {754974721ull, 469762049ull, 167772161ull};
-const uint64_t kG32[3] = {11, 3, 3};
+const uint64_t kP32[3] = {469762049ull, 167772161ull, 754974721ull};
+const uint64_t kG32[3] = {3, 3, 11};
 
 int v2(uint64_t x) {
     int k = 0;
@@ -269,6 +271,7 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     pd.log_c = pl->log_c;
     pd.lo = pl->lo;
     pd.log_cb = pl->log_cb;
+    pd.log_cb1 = pl->log_cb1;
     pd.tw_smem_r = pl->tw_smem_r;
     pd.log_fa = pl->log_c / 2;
     pd.log_r2 = pl->log_r2;
@@ -313,12 +316,13 @@ int bw_check_size(int path, int K, size_t la, size_t lb, int* log_n_out) {
     return BW_OK;
 }
 
-// BW_PATH_AUTO: the 32-bit path while its transform has at most 2^21 points
-// (its butterflies are cheaper, and on a B200 it measured 25-30% faster up
-// to 2^24-bit operands), the 64-bit path beyond (half the transform length,
-// faster once the transforms leave L2) and wherever the 32-bit path cannot
-// hold the product.
-constexpr int kAutoP32MaxLogN = 21;
+// BW_PATH_AUTO: the 32-bit path while its transform has at most 2^24 points
+// (its 32-bit butterflies are about four times cheaper than the 64-bit ones,
+// which more than pays for its doubled transform length: on a B200 it
+// measured 10-30% faster from 2^14- to 2^27-bit operands), the 64-bit path
+// beyond (at 2^28 bits the two measured equal) and wherever the 32-bit path
+// cannot hold the product.
+constexpr int kAutoP32MaxLogN = 24;
 
 int bw_choose_path(int K, size_t la, size_t lb) {
     int log_n = 0;
@@ -400,6 +404,22 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         const unsigned sms = mode == 2 ? sm_count() : 0u;
         while (log_cb > min_cb && (2u << (log_cols_outer - log_cb)) < 2u * sms) --log_cb;
         pl->log_cb = log_cb;
+        // forward column pass: its tile also stages the coefficients (16-bit
+        // halves as u16 on the 32-bit path, 32-bit limbs on the 64-bit path);
+        // residues + coefficients (+ staged twiddles) within 112 KiB keep two
+        // CTAs on an SM
+        pl->tw_smem_r =
+            ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
+        const size_t cbytes = path == BW_PATH_P32 ? 2 : 4;
+        const size_t tsb = pl->tw_smem_r ? ((size_t)2 * w << pl->log_r) : 0;
+        auto fits1 = [&](int cb) {
+            const size_t elems = (size_t)1 << (pl->log_r + cb);
+            return (w + cbytes) * elems + tsb <= (wide ? 196608 : 114688);
+        };
+        int log_cb1 = 0;
+        while (log_cb1 < log_cols_outer && fits1(log_cb1 + 1)) ++log_cb1;
+        while (log_cb1 > min_cb && (2u << (log_cols_outer - log_cb1)) < 2u * sms) --log_cb1;
+        pl->log_cb1 = log_cb1;
         if (pl->log_r2) {
             int l2 = 0;
             while (l2 < pl->log_c && ((size_t)w << (pl->log_r2 + l2 + 1)) <= 65536) ++l2;
@@ -408,8 +428,6 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         // column stage twiddles: read through L1 by default (measured faster
         // than staging them in shared memory, which costs occupancy); staged on
         // request when they take <= 32 KiB
-        pl->tw_smem_r =
-            ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
         pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
         pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
         pl->lo_out = (log_n + 1) / 2;
@@ -708,9 +726,10 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const bool ts = pl->tw_smem_r != 0;
     const size_t tw_bytes = ts ? (size_t)R * sizeof(Tw<T>) : 0;
 
-    const size_t smem1 = tw_bytes + (size_t)R * CB * sizeof(T) + (size_t)R * CB * 4;
+    const int CB1 = 1 << pl->log_cb1;
+    const size_t smem1 = tw_bytes + (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : 4));
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
-    dim3 g1(cols_outer / CB, 1, square ? 1 : 2);
+    dim3 g1(cols_outer / CB1, 1, square ? 1 : 2);
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     if (ts) {
         k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(

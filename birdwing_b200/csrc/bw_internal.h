@@ -9,6 +9,7 @@ struct bw_plan {
     int path = 0, K = 0;
     size_t la = 0, lb = 0, nca = 0, ncb = 0;
     int log_n = 0, log_r = 0, log_c = 0, log_cb = 0, lo = 0;
+    int log_cb1 = 0;     // forward column pass tile width (its own shared-memory budget)
     int tw_smem_r = 0;   // column stage twiddles staged in shared memory
     int rlog_row = 4;    // radix of the row kernel's rounds (2^3 or 2^4)
     int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)

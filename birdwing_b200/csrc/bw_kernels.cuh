@@ -35,6 +35,7 @@
 // three carry kernels (src/carry_prop.cu:8-211).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include "bw_arith.cuh"
 
 namespace bw {
@@ -83,7 +84,8 @@ struct PlanDev {
     GarnerDev<Ar> gar;
     int K;
     int log_n, log_r, log_c, lo;  // lo: split of the row-level twiddle exponent
-    int log_cb;                   // outer column tile width CB = 2^log_cb
+    int log_cb;                   // outer column tile width CB = 2^log_cb (inverse pass)
+    int log_cb1;                  // forward column pass tile width
     int tw_smem_r;                // stage the R-point twiddles in shared memory
     int log_fa;                   // per-row twiddle split a (F has 2^a entries)
     // three-pass schedule (n = R * R2 * C): log_r2 > 0, otherwise 0
@@ -302,16 +304,18 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                                              unsigned char* smem_raw) {
     using T = typename Ar::T;
     const bool zt = zt_in && P.log_r > 0;
-    const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb;
+    const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb1;
     const int R = 1 << log_r, CB = 1 << log_cb;
     const size_t C = (size_t)1 << log_c;  // stride between rows (R2 * C columns)
     const size_t n = (size_t)R * C;
     const int c0 = tile << log_cb;
     const int rows_loaded = zt ? R / 2 : R;
+    // staged coefficients: 16-bit halves (32-bit path) or 32-bit limbs
+    using CT = typename std::conditional<SPLIT16, uint16_t, uint32_t>::type;
 
     Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
     T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
-    uint32_t* coef = reinterpret_cast<uint32_t*>(buf + (R << log_cb));
+    CT* coef = reinterpret_cast<CT*>(buf + (R << log_cb));
 
     for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
         const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
@@ -323,7 +327,7 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                 val = __ldg(limbs + ci);
             }
         }
-        coef[e] = val;
+        coef[e] = (CT)val;
     }
 
     const int nr = sched_rounds<RLOG>(log_r);

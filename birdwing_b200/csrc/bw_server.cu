@@ -671,12 +671,10 @@ extern "C" int bw_server_prewarm(bw_server* s, int path, int max_log_n) {
     if (path == BW_PATH_AUTO) path = s->default_path;
     if (path != BW_PATH_AUTO && path != BW_PATH_P32 && path != BW_PATH_P64)
         return bw_fail(BW_EINVAL, "bad path");
-    // AUTO: the 32-bit path's lengths that automatic choice uses, and the
-    // 64-bit path's up to max_log_n
+    // AUTO: both paths' lengths up to max_log_n
     for (const int pth : {BW_PATH_P32, BW_PATH_P64}) {
         if (path != BW_PATH_AUTO && path != pth) continue;
         int top = std::min(max_log_n, std::min(kMaxGroupLogN, bw_path_max_log_n(pth, s->K)));
-        if (path == BW_PATH_AUTO && pth == BW_PATH_P32) top = std::min(top, 21);
         for (int ln = 4; ln <= top; ++ln) {
             bw_plan* pl = nullptr;
             const int rc = get_plan(s, pth, ln, &pl);

@@ -20,7 +20,7 @@ vector<TestDataTypeUint> roots_of_unity_max = {0, 0, 0};
 vector<TestDataTypeUint> moduli = {0x2aaaaa9500000001ULL, 0x2aaaaa8f00000001ULL};
 vector<TestDataTypeUint> roots_of_unity_max = {0, 0};
 #else
-vector<TestDataTypeUint> moduli = {754974721u, 469762049u, 167772161u};
+vector<TestDataTypeUint> moduli = {469762049u, 167772161u, 754974721u};
 vector<TestDataTypeUint> roots_of_unity_max = {0, 0, 0};
 #endif
 

@@ -160,8 +160,8 @@ int bw_size_supported(int path, int num_primes, size_t la, size_t lb);
 
 /* Build the plan (twiddle tables on the device, Garner constants) for
  * products of la x lb u32 words.  path = BW_PATH_AUTO picks the faster path
- * for the size: the 32-bit path while its transform has at most 2^21 points
- * (operands up to about 2^24 bits), the 64-bit path beyond; num_primes = 0
+ * for the size: the 32-bit path while its transform has at most 2^24 points
+ * (operands up to about 2^27 bits), the 64-bit path beyond; num_primes = 0
  * picks K = 2.  The plan is bound to the current CUDA device. */
 int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb,
                    int num_primes, unsigned flags);

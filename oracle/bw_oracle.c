@@ -400,8 +400,8 @@ done:
  * generator of the multiplicative group. */
 static const uint64_t P64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
 static const uint64_t G64[3] = {10, 7, 3};
-static const uint64_t P32[3] = {754974721ull, 469762049ull, 167772161ull};
-static const uint64_t G32[3] = {11, 3, 3};
+static const uint64_t P32[3] = {469762049ull, 167772161ull, 754974721ull};
+static const uint64_t G32[3] = {3, 3, 11};
 
 int oracle_path_basis(int path, uint64_t* primes, uint64_t* roots_max, int* max_logs) {
     const uint64_t* P = path == 64 ? P64 : P32;

@@ -36,15 +36,17 @@ def test_limits():
     l64 = bw.limits(bw.BW_PATH_P64)
     l32 = bw.limits(bw.BW_PATH_P32)
     assert l64["max_log_n"] == 32 and l64["num_primes"] == 2
-    assert l32["max_log_n"] == 24
-    assert l32["max_square_words"] == (1 << 23) // 2
+    assert l32["max_log_n"] == 25
+    assert l32["max_square_words"] == (1 << 24) // 2
+    assert bw.limits(bw.BW_PATH_P32, 3)["max_log_n"] == 24
     assert bw.limits(bw.BW_PATH_P64, 3)["num_primes"] == 3
 
 
 @pytest.mark.parametrize("la,lb,path,ok", [
     (1, 1, 64, True), (1 << 23, 1 << 23, 64, True), (1 << 28, 1 << 28, 64, True),
     (1 << 31, 1 << 31, 64, True), (1 << 32, 1 << 32, 64, False), (1 << 15, 1 << 15, 32, True),
-    (1 << 23, 1 << 23, 32, False),   # 2^24 16-bit coefficients each -> n = 2^25
+    (1 << 23, 1 << 23, 32, True),    # 2^24 16-bit coefficients each -> n = 2^25
+    (1 << 24, 1 << 23, 32, False),   # n = 2^26 is beyond the 32-bit path
     (0, 5, 64, False), (5, 0, 32, False),
 ])
 def test_size_supported(la, lb, path, ok):
