@@ -146,6 +146,23 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Asynchronous global -> shared copy of one element (cp.async): a tile's
+// loads are all issued at once and land while the CTA builds its twiddle
+// tables; the issuing thread waits for its own copies with cp_async_wait.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (sizeof(T) == 8) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // Round schedule of a 2^log_len-point transform with rounds of up to RLOG
 // stages: the remainder round comes first, where the sub-problem stride is
 // largest and shared-memory accesses are conflict-free.  Computed
@@ -319,16 +336,20 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
 
     for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
         const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
-        uint32_t val = 0;
-        if (ci < ncoef) {
-            if constexpr (SPLIT16) {
-                val = (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu;
+        if constexpr (SPLIT16) {
+            const uint32_t val =
+                ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu : 0u;
+            coef[e] = (CT)val;
+        } else {
+            // 32-bit limbs land in shared memory without passing registers
+            if (ci < ncoef) {
+                cp_async_elem(coef + e, limbs + ci);
             } else {
-                val = __ldg(limbs + ci);
+                coef[e] = 0;
             }
         }
-        coef[e] = (CT)val;
     }
+    if constexpr (!SPLIT16) cp_async_wait();
 
     const int nr = sched_rounds<RLOG>(log_r);
     for (int kp = 0; kp < P.K; ++kp) {
@@ -456,6 +477,8 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     }
     __syncthreads();
 
+    // (loading the rows by cp.async during the table build measured slower:
+    // the in-place twiddle then costs one more shared-memory pass)
     for (int i = threadIdx.x; i < C; i += NT) {
         const Tw<T> f = F[i & (nf - 1)], g = G[i >> la];
         bufA[swz<T>(i)] = ar.mulc(ar.mulc(ga[i], f.w, f.wq), g.w, g.wq);
@@ -592,6 +615,12 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
     Tw<T>* Tcol = Trow + R2;                             // CB entries
     T* buf = reinterpret_cast<T*>(Tcol + CB);
 
+    if constexpr (!INV) {
+        // the tile's loads first: they land while the twiddle tables are built
+        for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x)
+            cp_async_elem(buf + swz<T>(e), g + ((size_t)(e >> log_cb) << log_c) + c0 +
+                                               (e & (CB - 1)));
+    }
     const uint64_t k1 = bitrev((uint32_t)s, P.log_r);
     const uint64_t nmask = n - 1;
     for (int i = threadIdx.x; i < R2 + CB; i += blockDim.x) {
@@ -605,6 +634,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
             Tcol[i - R2] = t;
         }
     }
+    if constexpr (!INV) cp_async_wait();  // this thread's elements
     __syncthreads();
 
     const int nr = sched_rounds<RLOG>(log_r2);
@@ -612,8 +642,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
         for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x) {
             const int i2 = e >> log_cb, v = e & (CB - 1);
             const Tw<T> a = Tcol[v], b = Trow[i2];
-            buf[swz<T>(e)] = ar.mulc(ar.mulc(g[((size_t)i2 << log_c) + c0 + v], a.w, a.wq),
-                                      b.w, b.wq);
+            buf[swz<T>(e)] = ar.mulc(ar.mulc(buf[swz<T>(e)], a.w, a.wq), b.w, b.wq);
         }
         __syncthreads();
         for (int r = 0; r < nr; ++r) {
