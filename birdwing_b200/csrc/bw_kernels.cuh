@@ -615,12 +615,9 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
     Tw<T>* Tcol = Trow + R2;                             // CB entries
     T* buf = reinterpret_cast<T*>(Tcol + CB);
 
-    if constexpr (!INV) {
-        // the tile's loads first: they land while the twiddle tables are built
-        for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x)
-            cp_async_elem(buf + swz<T>(e), g + ((size_t)(e >> log_cb) << log_c) + c0 +
-                                               (e & (CB - 1)));
-    }
+    // the tile's loads first: they land while the twiddle tables are built
+    for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x)
+        cp_async_elem(buf + swz<T>(e), g + ((size_t)(e >> log_cb) << log_c) + c0 + (e & (CB - 1)));
     const uint64_t k1 = bitrev((uint32_t)s, P.log_r);
     const uint64_t nmask = n - 1;
     for (int i = threadIdx.x; i < R2 + CB; i += blockDim.x) {
@@ -634,7 +631,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
             Tcol[i - R2] = t;
         }
     }
-    if constexpr (!INV) cp_async_wait();  // this thread's elements
+    cp_async_wait();  // this thread's elements
     __syncthreads();
 
     const int nr = sched_rounds<RLOG>(log_r2);
@@ -662,11 +659,8 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
         }
     } else {
         for (int r = nr - 1; r >= 0; --r) {
-            const bool first = (r == nr - 1), last = (r == 0);
-            auto ld = [&](int v, int idx) -> T {
-                if (first) return g[((size_t)idx << log_c) + c0 + v];
-                return buf[swz<T>((idx << log_cb) + v)];
-            };
+            const bool last = (r == 0);
+            auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
             auto st = [&](int v, int idx, T val) {
                 if (last) {
                     const Tw<T> a = Tcol[v], b = Trow[idx];
@@ -711,14 +705,17 @@ __device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::
         __syncthreads();
     }
 
+    // the whole tile in flight at once (cp.async), then every round from
+    // shared memory; the last round reduces and writes global memory
+    for (int e = threadIdx.x; e < (R << log_cb); e += blockDim.x)
+        cp_async_elem(buf + swz<T>(e), g + (size_t)(e >> log_cb) * C + c0 + (e & ((1 << log_cb) - 1)));
+    cp_async_wait();
+    __syncthreads();
+
     const int nr = sched_rounds<RLOG>(log_r);
     for (int r = nr - 1; r >= 0; --r) {
-        const bool first = (r == nr - 1), last = (r == 0);
-        // first round reads global memory, last round reduces and writes it
-        auto ld = [&](int v, int idx) -> T {
-            if (first) return g[(size_t)idx * C + c0 + v];
-            return buf[swz<T>((idx << log_cb) + v)];
-        };
+        const bool last = (r == 0);
+        auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
         auto st = [&](int v, int idx, T val) {
             if (last) {
                 g[(size_t)idx * C + c0 + v] = ar.inv_out(val);
