@@ -369,3 +369,22 @@ def test_device_pointer_graph_replay(path, K, la, lb):
             c.sync()
             got = out.cpu().numpy().view(np.uint32)
             assert (got == gmp_ref.mul(a, b)).all(), it
+
+
+def test_p32_longest_transform_vs_gmp():
+    # the 32-bit path at its longest transform (2^25 points, K = 2): two
+    # 2^28-bit operands split into 16-bit coefficients, against GMP
+    a = mt64.random_words_top_fast(1 << 23, 99)
+    b = mt64.random_words_top_fast(1 << 23, 98)
+    with bw.Plan(a.size, b.size, 32, 2) as p, bw.Context(p) as c:
+        assert p.info["log_n"] == 25
+        got = c.multiply(a, b)
+    assert (got == gmp_ref.mul(a, b)).all()
+
+
+def test_automatic_path_choice():
+    # 32-bit path while its transform has at most 2^24 points, 64-bit beyond
+    for la, lb, want in [(1, 1, 32), (1000, 700, 32), (1 << 22, 1 << 22, 32),
+                         (1 << 22, (1 << 22) + 1, 64), (1 << 23, 1 << 23, 64)]:
+        with bw.Plan(la, lb) as p:
+            assert p.info["path"] == want, (la, lb, p.info["path"])
