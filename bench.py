@@ -561,7 +561,7 @@ def bench_batch(args):
             "clocks": clocks,
             "tune_table": bw.tune_table() if args.autotune else None,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:   # the CPU baseline runs at N = 1 only
             line["cpu_baseline"] = cpu_baseline_items(items, K)
         print(json.dumps(line))
     bt.close()
@@ -816,7 +816,7 @@ def bench_serving(args):
             "gpu_launches": st["kernel_launches"] - st0["kernel_launches"],
             "clocks": clocks,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:   # the CPU baseline runs at N = 1 only
             line["cpu_baseline"] = cpu_baseline_items([(64, a, b) for a, b in pool], K)
         print(json.dumps(line))
     if world > 1:
@@ -1057,7 +1057,7 @@ def main():
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:   # the CPU baseline runs at N = 1 only
             line["cpu_baseline"] = cpu_baseline(args.config)
         print(json.dumps(line))
     ctx.close()
