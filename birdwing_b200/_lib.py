@@ -136,6 +136,8 @@ SIGNATURES = {
     "bw_batch_run": (_I, [_P, _U, ctypes.POINTER(bw_timing)]),
     "bw_batch_get_info": (_I, [_P, ctypes.POINTER(bw_batch_info)]),
     "bw_batch_autotune": (_I, [_P, _I]),
+    "bw_batch_set_wait_limit": (_I, [_P, _I]),
+    "bw_batch_inject_wait_fault": (_I, [_P, _I]),
     "bw_tune_table_export": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "bw_tune_table_set": (_I, [_I, _I, _I, _I, _I]),
     "bw_server_create": (_I, [ctypes.POINTER(_P), ctypes.POINTER(bw_server_config)]),

@@ -286,6 +286,14 @@ class Batch:
     def autotune(self, reps=3):
         check(lib.bw_batch_autotune(self._h, reps))
 
+    def set_wait_limit(self, polls):
+        """Test hook: polls a look-back wait may take before BW_ETIMEOUT."""
+        check(lib.bw_batch_set_wait_limit(self._h, polls))
+
+    def inject_wait_fault(self, enable=True):
+        """Test hook: make every look-back wait of the 4-step groups run out."""
+        check(lib.bw_batch_inject_wait_fault(self._h, 1 if enable else 0))
+
     def close(self):
         if self._h:
             lib.bw_batch_destroy(self._h)

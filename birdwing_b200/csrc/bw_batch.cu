@@ -135,6 +135,8 @@ struct bw_batch {
     cudaEvent_t fork = nullptr, join[kSide] = {};
     cudaEvent_t ev[4] = {};
     size_t graph_nodes = 0;
+    int spin_limit = 1 << 22;
+    bool inject_wait_fault = false;
 };
 
 namespace {
@@ -203,7 +205,7 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
     const size_t smem3 = (size_t)R * CB * sizeof(T);
     kb_inv_col<Ar, 4><<<dim3(C / CB, pl.K, np), kColThreads, smem3, s>>>(P, g.d_desc, ra);
     kb_garner_carry<Ar, SPLIT16><<<dim3((unsigned)g.ntiles, np), kCarryThreads, 0, s>>>(
-        P, g.d_desc, ra, 1u, g.d_err, g.spin_limit);
+        P, g.d_desc, ra, 1u, g.inject_wait_fault ? 1u + (1u << 27) : 1u, g.d_err, g.spin_limit);
 }
 
 int set_group_attrs() {
@@ -401,7 +403,8 @@ int build_layout(bw_batch* bt) {
     for (size_t i = 0; i < order.size() && rc == BW_OK; ++i) {
         const Bucket& bk = bt->buckets[order[i]];
         bw_group_launch g{&bk.plan, bk.d_desc, (unsigned)bk.prods.size(), bk.d_res_a,
-                          bk.d_res_b, bk.ntiles, bt->d_err, 1 << 22};
+                          bk.d_res_b, bk.ntiles, bt->d_err, bt->spin_limit,
+                          bt->inject_wait_fault};
         rc = bw_enqueue_group(g, bt->side[i % nside]);
     }
     for (int s = 0; s < nside; ++s) {
@@ -558,6 +561,22 @@ extern "C" int bw_batch_run(bw_batch* bt, unsigned what, bw_timing* tm) {
     const uint32_t err = *bt->h_err;
     if (err & 1u) return bw_fail(BW_ETIMEOUT, "carry look-back wait exceeded its bound");
     if (err) return bw_fail(BW_ECHECK, "redundant-prime reconstruction check failed");
+    return BW_OK;
+}
+
+extern "C" int bw_batch_set_wait_limit(bw_batch* bt, int polls) {
+    bw_clear_error();
+    if (!bt || polls < 0) return bw_fail(BW_EINVAL, "bad argument");
+    bt->spin_limit = polls;
+    bt->dirty = true;  // the limit is a launch argument of the captured graph
+    return BW_OK;
+}
+
+extern "C" int bw_batch_inject_wait_fault(bw_batch* bt, int enable) {
+    bw_clear_error();
+    if (!bt) return bw_fail(BW_EINVAL, "NULL batch");
+    bt->inject_wait_fault = enable != 0;
+    bt->dirty = true;
     return BW_OK;
 }
 

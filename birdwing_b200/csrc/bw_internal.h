@@ -52,6 +52,7 @@ struct bw_group_launch {
     size_t ntiles;      // carry tiles per product (bw_group_ntiles)
     uint32_t* d_err;    // bit 0: look-back wait timed out; bit 1: check failed
     int spin_limit;
+    bool inject_wait_fault = false;  // test hook: every look-back wait runs out
 };
 int bw_enqueue_group(const bw_group_launch& g, cudaStream_t s);
 // Carry tiles of a group whose longest product has max_words output words.

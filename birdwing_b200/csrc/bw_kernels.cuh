@@ -1101,12 +1101,12 @@ k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
 template <class Ar, bool SPLIT16>
 __global__ void __launch_bounds__(kCarryThreads, 4)
 kb_garner_carry(const PlanDev<Ar> P, const BatchProd* __restrict__ D,
-                const typename Ar::T* __restrict__ res_a, uint32_t epoch,
+                const typename Ar::T* __restrict__ res_a, uint32_t epoch, uint32_t wait_epoch,
                 uint32_t* __restrict__ err, int spin_limit) {
     const BatchProd d = D[blockIdx.y];
     const size_t NL = ((size_t)1 << P.log_n) / (SPLIT16 ? 2 : 1);
     garner_carry_body<Ar, SPLIT16>(P, res_a + d.res_off, d.out, (size_t)d.la + d.lb, NL, d.cst,
-                                   d.rec_x, d.rec_s, epoch, epoch, err, spin_limit);
+                                   d.rec_x, d.rec_s, epoch, wait_epoch, err, spin_limit);
 }
 
 // ------------------------------------------------------------------ small products

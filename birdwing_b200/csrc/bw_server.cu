@@ -383,7 +383,8 @@ int launch_group(bw_server* s, Group* g) {
                        small ? nullptr : g->dmem + rb_off,
                        ntiles,
                        reinterpret_cast<uint32_t*>(g->dmem + g->err_off),
-                       1 << 22};
+                       1 << 22,
+                       false};
     rc = bw_enqueue_group(gl, st);
     if (rc) return rc;
     e = cudaGetLastError();

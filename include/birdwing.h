@@ -290,6 +290,12 @@ int bw_batch_add(bw_batch* batch, int path, const uint32_t* a, size_t la,
  * total_ms.  BW_ECHECK / BW_ETIMEOUT as for bw_multiply. */
 int bw_batch_run(bw_batch* batch, unsigned what, bw_timing* timing);
 int bw_batch_get_info(const bw_batch* batch, bw_batch_info* info);
+/* Test hooks for the bounded look-back waits of the 4-step groups, as for
+ * contexts (bw_ctx_set_wait_limit / bw_ctx_inject_wait_fault): a run with the
+ * fault injected reports BW_ETIMEOUT, and the batch is correct again once
+ * it is switched off.  Both rebuild the captured graph at the next run. */
+int bw_batch_set_wait_limit(bw_batch* batch, int polls);
+int bw_batch_inject_wait_fault(bw_batch* batch, int enable);
 
 /* Time each candidate form of each group (one CTA per product where the
  * transform fits shared memory; 4-step with three column/row splits) on the

@@ -204,3 +204,24 @@ def test_uneven_mix_vs_gmp():
     assert info["products"] == 4096
     for (p, a, b), got in zip(mix, outs):
         assert (got == gmp_ref.mul(a, b)).all(), (p, len(a), len(b))
+
+
+def test_lookback_wait_fault_is_reported_and_recoverable():
+    # the 4-step groups' carry look-back waits are bounded: with the fault
+    # injected (every wait looks for a record nobody writes) the run reports
+    # BW_ETIMEOUT, and the same batch is correct once it is switched off
+    rng = np.random.default_rng(44)
+    items = [(64, rand_words(30000, rng), rand_words(9000, rng)) for _ in range(3)]
+    items += [(32, rand_words(20000, rng), rand_words(20000, rng)) for _ in range(3)]
+    with bw.Batch() as bt:
+        outs = [bt.add(a, b, path=p) for p, a, b in items]
+        bt.set_wait_limit(2000)
+        bt.inject_wait_fault(True)
+        with pytest.raises(bw.BwError) as ei:
+            bt.run()
+        assert ei.value.code == bw._lib.BW_ETIMEOUT
+        bt.inject_wait_fault(False)
+        bt.set_wait_limit(1 << 22)
+        bt.run()
+        for (p, a, b), got in zip(items, outs):
+            assert (got == gmp_ref.mul(a, b)).all()
