@@ -25,6 +25,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -100,6 +101,29 @@ struct Bucket {
     size_t ntiles = 0;
 };
 
+// Host staging copies of a batch (operands into pinned memory, results out of
+// it) split over a few threads: one thread's memcpy bandwidth bounded the
+// batch's end-to-end rate.
+template <class F>
+void parallel_products(size_t lo, size_t hi, size_t bytes, F fn) {
+    const size_t count = hi - lo;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>({8, hw, std::max<size_t>(1, bytes >> 22), count});
+    if (nt <= 1) {
+        for (size_t i = lo; i < hi; ++i) fn(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (size_t i = lo + t * count / nt; i < lo + (t + 1) * count / nt; ++i) fn(i);
+        });
+    for (auto& x : th) x.join();
+}
+
+// The staging copies and the DMA overlap chunk by chunk.
+constexpr size_t kStageChunks = 4;
+
 void free_bucket(Bucket& b) {
     cudaFree(b.d_desc);
     cudaFree(b.d_res_a);
@@ -134,6 +158,7 @@ struct bw_batch {
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
     cudaEvent_t ev[4] = {};
+    cudaEvent_t chunk_ev[kStageChunks] = {};
     size_t graph_nodes = 0;
     int spin_limit = 1 << 22;
     bool inject_wait_fault = false;
@@ -456,6 +481,8 @@ extern "C" int bw_batch_create(bw_batch** out, void* stream, unsigned flags) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming);
     for (auto& ev : bt->ev)
         if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    for (auto& ev : bt->chunk_ev)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&bt->d_err, 16);
     if (e == cudaSuccess) e = cudaMallocHost(&bt->h_err, 16);
     if (e != cudaSuccess) return fail(bw_fail(BW_ECUDA, "batch setup: %s", cudaGetErrorString(e)));
@@ -479,6 +506,8 @@ extern "C" int bw_batch_destroy(bw_batch* bt) {
     }
     if (bt->fork) cudaEventDestroy(bt->fork);
     for (auto& ev : bt->ev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : bt->chunk_ev)
         if (ev) cudaEventDestroy(ev);
     if (bt->own_stream && bt->stream) cudaStreamDestroy(bt->stream);
     delete bt;
@@ -531,26 +560,55 @@ extern "C" int bw_batch_run(bw_batch* bt, unsigned what, bw_timing* tm) {
         if (rc) return rc;
         what |= BW_BATCH_UPLOAD;  // the staging arenas were (re)built
     }
+    const size_t np = bt->prods.size();
+    auto chunk = [&](size_t c) { return c * np / kStageChunks; };
     cudaEventRecord(bt->ev[0], bt->stream);
     if (what & BW_BATCH_UPLOAD) {
-        for (const Prod& p : bt->prods) {
-            memcpy(bt->h_in + p.in_a, p.a, p.la * 4);
-            if (!p.square) memcpy(bt->h_in + p.in_b, p.b, p.lb * 4);
+        // chunk c's DMA runs while the host stages chunk c + 1
+        for (size_t c = 0; c < kStageChunks; ++c) {
+            const size_t lo = chunk(c), hi = chunk(c + 1);
+            if (lo == hi) continue;
+            const size_t w_lo = bt->prods[lo].in_a;
+            const size_t w_hi = hi < np ? bt->prods[hi].in_a : bt->in_words;
+            parallel_products(lo, hi, (w_hi - w_lo) * 4, [&](size_t i) {
+                const Prod& p = bt->prods[i];
+                memcpy(bt->h_in + p.in_a, p.a, p.la * 4);
+                if (!p.square) memcpy(bt->h_in + p.in_b, p.b, p.lb * 4);
+            });
+            BW_TRY(cudaMemcpyAsync(bt->d_in + w_lo, bt->h_in + w_lo, (w_hi - w_lo) * 4,
+                                   cudaMemcpyHostToDevice, bt->stream));
         }
-        BW_TRY(cudaMemcpyAsync(bt->d_in, bt->h_in, bt->in_words * 4, cudaMemcpyHostToDevice,
-                               bt->stream));
     }
     cudaEventRecord(bt->ev[1], bt->stream);
     if (what & BW_BATCH_COMPUTE) BW_TRY(cudaGraphLaunch(bt->exec, bt->stream));
     cudaEventRecord(bt->ev[2], bt->stream);
-    if (what & BW_BATCH_DOWNLOAD)
-        BW_TRY(cudaMemcpyAsync(bt->h_out, bt->d_out, bt->out_words * 4, cudaMemcpyDeviceToHost,
-                               bt->stream));
+    if (what & BW_BATCH_DOWNLOAD) {
+        for (size_t c = 0; c < kStageChunks; ++c) {
+            const size_t lo = chunk(c), hi = chunk(c + 1);
+            if (lo == hi) continue;
+            const size_t w_lo = bt->prods[lo].out;
+            const size_t w_hi = hi < np ? bt->prods[hi].out : bt->out_words;
+            BW_TRY(cudaMemcpyAsync(bt->h_out + w_lo, bt->d_out + w_lo, (w_hi - w_lo) * 4,
+                                   cudaMemcpyDeviceToHost, bt->stream));
+            BW_TRY(cudaEventRecord(bt->chunk_ev[c], bt->stream));
+        }
+    }
     BW_TRY(cudaMemcpyAsync(bt->h_err, bt->d_err, 4, cudaMemcpyDeviceToHost, bt->stream));
     cudaEventRecord(bt->ev[3], bt->stream);
+    if (what & BW_BATCH_DOWNLOAD) {
+        // the host copies chunk c out while chunk c + 1 is still in flight
+        for (size_t c = 0; c < kStageChunks; ++c) {
+            const size_t lo = chunk(c), hi = chunk(c + 1);
+            if (lo == hi) continue;
+            BW_TRY(cudaEventSynchronize(bt->chunk_ev[c]));
+            const size_t w_hi = hi < np ? bt->prods[hi].out : bt->out_words;
+            parallel_products(lo, hi, (w_hi - bt->prods[lo].out) * 4, [&](size_t i) {
+                const Prod& p = bt->prods[i];
+                memcpy(p.c, bt->h_out + p.out, (p.la + p.lb) * 4);
+            });
+        }
+    }
     BW_TRY(cudaStreamSynchronize(bt->stream));
-    if (what & BW_BATCH_DOWNLOAD)
-        for (const Prod& p : bt->prods) memcpy(p.c, bt->h_out + p.out, (p.la + p.lb) * 4);
     if (tm) {
         memset(tm, 0, sizeof *tm);
         tm->h2d_ms = elapsed(bt->ev[0], bt->ev[1]);
