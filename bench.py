@@ -980,6 +980,15 @@ def main():
         ctx.multiply(ha, hb, out=hc)
         e2e_ms.append(1000 * (time.perf_counter() - t0))
     e2e_block_total = reduce_over_ranks([sum(e2e_ms)], ["max"])[0]
+    # blocking from pageable numpy arrays: the drop-in host_multiply_merge case
+    pc = np.empty(la + lb, dtype=np.uint32)
+    ctx.multiply(a, b, out=pc)
+    e2e_pg = []
+    for _ in range(min(args.e2e_steps, 3)):
+        t0 = time.perf_counter()
+        ctx.multiply(a, b, out=pc)
+        e2e_pg.append(1000 * (time.perf_counter() - t0))
+    e2e_pg_total = reduce_over_ranks([sum(e2e_pg)], ["max"])[0]
     # pipelined: two contexts used in turn (BW_PTR_HOST_ASYNC), so one
     # product's copies overlap the other's kernels; every product still
     # copies its operands in and its result out
@@ -1053,6 +1062,8 @@ def main():
                     "how": "bw_multiply(BW_PTR_HOST_ASYNC) on three contexts in turn from "
                            "pinned host buffers; wall clock over all steps",
                     "blocking_value": job_throughput(args.e2e_steps, world, e2e_block_total),
+                    "blocking_pageable_value": job_throughput(min(args.e2e_steps, 3), world,
+                                                              e2e_pg_total),
                     "correct_vs_gmp": ok_e2e},
             "gpu_launches": 5 * args.steps,
             "clocks": clocks,
