@@ -121,12 +121,15 @@ def write_csv(path, rows, append=False):
 def measure(pipeline, L_arg, warmup=2, iters=5, seed=1234):
     """Time one size through the C ABI: setup (pin, plan, context), iters
     blocking products from pinned host buffers with per-stage events, and
-    teardown.  The last product is checked before the row is returned."""
+    teardown.  The last product is checked before the row is returned.
+    None when the pipeline's primes do not reach this size."""
     import torch
 
     import birdwing_b200 as bw
     path, limb_bits = PIPELINES[pipeline]
     words = resolve_limbs(L_arg) * limb_bits // 32
+    if not bw.size_supported(words, words, path):
+        return None
     rng = np.random.default_rng(seed)
     a = rng.integers(0, 1 << 32, words, dtype=np.uint64).astype(np.uint32)
     b = rng.integers(0, 1 << 32, words, dtype=np.uint64).astype(np.uint32)
@@ -177,7 +180,13 @@ def main(argv=None):
     ap.add_argument("--csv", default="gpu_full_multiply.csv")
     ap.add_argument("--append", action="store_true")
     args = ap.parse_args(argv)
-    rows = [measure(args.pipeline, int(x), args.warmup, args.iters) for x in args.L.split(",")]
+    rows = []
+    for x in args.L.split(","):
+        r = measure(args.pipeline, int(x), args.warmup, args.iters)
+        if r is None:
+            print(f"{args.pipeline:>7} L_arg={x}: beyond this pipeline's transform length")
+        else:
+            rows.append(r)
     write_csv(args.csv, rows, args.append)
     for r in rows:
         print(f"{r['pipeline']:>7} L={r['L']:>9} N=2^{r['logN']:<2} mean {r['mean_ms']:.3f} ms")
