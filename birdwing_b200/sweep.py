@@ -128,7 +128,7 @@ def measure(pipeline, L_arg, warmup=2, iters=5, seed=1234):
     import birdwing_b200 as bw
     path, limb_bits = PIPELINES[pipeline]
     words = resolve_limbs(L_arg) * limb_bits // 32
-    if not bw.size_supported(words, words, path):
+    if not bw.size_supported(words, words, path)[0]:
         return None
     rng = np.random.default_rng(seed)
     a = rng.integers(0, 1 << 32, words, dtype=np.uint64).astype(np.uint32)
