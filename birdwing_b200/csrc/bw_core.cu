@@ -467,6 +467,7 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
         delete pl;
         return rc;
     }
+    pl->order = new bw_stage_order();
     *out = pl;
     return BW_OK;
 }
@@ -474,6 +475,7 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
 extern "C" int bw_plan_destroy(bw_plan* pl) {
     if (!pl) return BW_OK;
     if (pl->d_tables) cudaFree(pl->d_tables);
+    delete pl->order;
     delete pl;
     return BW_OK;
 }
@@ -533,6 +535,8 @@ struct bw_ctx {
     bool g_sq = false;
     uint32_t* h_err = nullptr;  // pinned
     cudaEvent_t ev[8] = {};
+    cudaEvent_t stage_ev[3] = {};  // ends of copy-in, kernels, copy-out (stage order)
+    bool counted = false;          // included in the plan's live contexts
     int spin_limit = 1 << 22;
     bool inject_wait_fault = false;
 };
@@ -583,6 +587,14 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
     for (auto& ev : c->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess)
             return fail(bw_fail(BW_ECUDA, "event: %s", cudaGetErrorString(e)));
+    for (auto& ev : c->stage_ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+            return fail(bw_fail(BW_ECUDA, "event: %s", cudaGetErrorString(e)));
+    if (pl->order) {
+        std::lock_guard<std::mutex> lk(pl->order->mu);
+        pl->order->contexts++;
+        c->counted = true;
+    }
     *out = c;
     return BW_OK;
 }
@@ -590,8 +602,20 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
 extern "C" int bw_ctx_destroy(bw_ctx* c) {
     if (!c) return BW_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->counted) {
+        bw_stage_order* so = c->plan->order;
+        std::lock_guard<std::mutex> lk(so->mu);
+        so->contexts--;
+        for (int i = 0; i < 3; ++i)
+            if (so->owner[i] == c) {
+                so->owner[i] = nullptr;
+                so->last[i] = nullptr;
+            }
+    }
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto& ev : c->ev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : c->stage_ev)
         if (ev) cudaEventDestroy(ev);
     if (c->h_err) cudaFreeHost(c->h_err);
     cudaFree(c->d_state);
@@ -906,18 +930,43 @@ static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* 
             BW_CUDA(cudaEventSynchronize(c->ev[6]));
         }
     } else {
+        // With several live contexts on the plan, each stage waits for the
+        // same stage of the plan's previous product (bw_stage_order).  The
+        // lock also keeps the three stages of one call together in that order.
+        bw_stage_order* so = pl->order;
+        std::unique_lock<std::mutex> lk;
+        if (so) lk = std::unique_lock<std::mutex>(so->mu);
+        const bool ordered = so && so->contexts > 1;
+        auto stage_begin = [&](int i) -> cudaError_t {
+            if (!ordered || !so->last[i] || so->owner[i] == c) return cudaSuccess;
+            return cudaStreamWaitEvent(c->stream, so->last[i], 0);
+        };
+        auto stage_end = [&](int i) -> cudaError_t {
+            if (!ordered) return cudaSuccess;
+            const cudaError_t e = cudaEventRecord(c->stage_ev[i], c->stream);
+            so->last[i] = c->stage_ev[i];
+            so->owner[i] = c;
+            return e;
+        };
+        BW_CUDA(stage_begin(0));
         BW_CUDA(cudaMemcpyAsync(c->d_in, a, la * 4, cudaMemcpyHostToDevice, c->stream));
         const uint32_t* db = c->d_in;
         if (!sq) {
             BW_CUDA(cudaMemcpyAsync(c->d_in + la, b, lb * 4, cudaMemcpyHostToDevice, c->stream));
             db = c->d_in + la;
         }
+        BW_CUDA(stage_end(0));
+        BW_CUDA(stage_begin(1));
         if (timing) cudaEventRecord(c->ev[1], c->stream);
         rc = enqueue_product(c, c->d_in, db, c->d_out, sq, timing);
         if (rc) return rc;
         if (timing) cudaEventRecord(c->ev[5], c->stream);
+        BW_CUDA(stage_end(1));
+        BW_CUDA(stage_begin(2));
         BW_CUDA(cudaMemcpyAsync(out, c->d_out, M * 4, cudaMemcpyDeviceToHost, c->stream));
+        BW_CUDA(stage_end(2));
         if (timing) cudaEventRecord(c->ev[6], c->stream);
+        if (lk.owns_lock()) lk.unlock();
         if (flags & BW_PTR_HOST_ASYNC) return BW_OK;  // bw_ctx_sync reports errors
         rc = read_device_errors(c);
         if (rc) return rc;

@@ -2,8 +2,23 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 
 #include "bw_kernels.cuh"
+
+// Stage order of the host-pointer products of one plan.  Contexts of one
+// plan used in turn form a three-stage pipeline (copy-in, kernels,
+// copy-out): each stage of a product waits for the same stage of the plan's
+// previous product, so every stage runs alone at full speed while the three
+// overlap.  Unordered, the products in flight share the PCIe link and the SMs
+// evenly and finish together, and the copies hide little of the kernels.
+// Only plans with more than one live context order their products.
+struct bw_stage_order {
+    std::mutex mu;
+    int contexts = 0;              // live contexts of the plan
+    cudaEvent_t last[3] = {};      // end of the previous product's stage i
+    const void* owner[3] = {};     // context that recorded last[i]
+};
 
 struct bw_plan {
     int path = 0, K = 0;
@@ -22,6 +37,7 @@ struct bw_plan {
     bw::PlanDev<bw::Ar32> pd32{};
     bw::PlanDev<bw::Ar64> pd64{};
     uint64_t primes[3] = {0, 0, 0};
+    bw_stage_order* order = nullptr;  // plans of bw_plan_create only
 };
 
 // Split, tables and constants of a plan for transform length 2^log_n.

@@ -345,6 +345,60 @@ def test_async_host_mode_two_contexts():
         assert (o == gmp_ref.mul(a, b)).all()
 
 
+@pytest.mark.gpu
+def test_stage_order_across_contexts():
+    """Three contexts of one plan form an ordered copy-in / kernels / copy-out
+    pipeline: products issued in turn (asynchronous, blocking with timing, and
+    squarings) stay exact, and a context whose events the plan's order
+    refers to can be destroyed while the others keep going."""
+    import torch
+    rng = np.random.default_rng(37)
+    la, lb = 70001, 65536
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    pairs = [(rand_words(la, rng), rand_words(lb, rng)) for _ in range(9)]
+    ins = [(pinned(a), pinned(b)) for a, b in pairs]
+    outs = [pinned(np.zeros(la + lb, dtype=np.uint32)) for _ in pairs]
+    with bw.Plan(la, lb, 64, 2) as p:
+        ctxs = [bw.Context(p) for _ in range(3)]
+        for i, ((a, b), o) in enumerate(zip(ins[:6], outs[:6])):
+            c = ctxs[i % 3]
+            if i >= 3:
+                c.sync()
+            c.multiply_async(a, b, o)
+        # the last issuer owns the plan's stage events: destroy it mid-stream
+        ctxs[2].close()
+        for i in range(6, 9):
+            c = ctxs[i % 2]
+            c.sync()
+            c.multiply_async(ins[i][0], ins[i][1], outs[i])
+        for c in ctxs[:2]:
+            c.sync()
+        # blocking calls with stage times, alternating contexts
+        for i in range(2):
+            got, t = ctxs[i].multiply(pairs[i][0], pairs[i][1], timing=True)
+            assert (got == gmp_ref.mul(*pairs[i])).all()
+            assert t["total_ms"] > 0
+        for c in ctxs[:2]:
+            c.close()
+    for (a, b), o in zip(pairs, outs):
+        assert (o == gmp_ref.mul(a, b)).all()
+    with bw.Plan(la, la, 32, 3) as p, bw.Context(p) as c0, bw.Context(p) as c1:
+        sq = [pinned(rand_words(la, rng)) for _ in range(4)]
+        so = [pinned(np.zeros(2 * la, dtype=np.uint32)) for _ in sq]
+        for i, (x, o) in enumerate(zip(sq, so)):
+            c = (c0, c1)[i % 2]
+            if i >= 2:
+                c.sync()
+            c.multiply_async(x, x, o)
+        c0.sync()
+        c1.sync()
+        for x, o in zip(sq, so):
+            assert (o == gmp_ref.mul(x, x)).all()
+
+
 @pytest.mark.parametrize("path,K,la,lb", [(64, 2, 70000, 50000), (32, 3, 3000, 2999),
                                           (64, 3, 5000, 1)])
 def test_device_pointer_graph_replay(path, K, la, lb):
