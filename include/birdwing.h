@@ -96,9 +96,13 @@ extern "C" {
                                 copy-in, product and copy-out on the context's
                                 stream and returns; the buffers must stay
                                 valid until bw_ctx_sync, which also reports
-                                device-side errors.  Two contexts used in turn
-                                overlap one product's copies with the other's
-                                kernels.  timing must be NULL.               */
+                                device-side errors.  Two or three contexts of
+                                one plan used in turn overlap one product's
+                                copies with another's kernels: host-pointer
+                                products of a plan with several live contexts
+                                run each stage (copy-in, kernels, copy-out)
+                                after the same stage of the plan's previous
+                                product.  timing must be NULL.               */
 
 /* Opaque handles.  A plan owns the per-size device tables (twiddles, Garner
  * constants); a context owns device scratch and a stream and borrows its
