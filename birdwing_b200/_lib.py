@@ -126,6 +126,7 @@ SIGNATURES = {
     "bw_multiply_coeffs": (_I, [_P, _P, _SZ, _P, _SZ, _P, _SZ]),
     "bw_garner_carry_noalloc": (_I, [_I, _I, _P, _SZ, _P, _SZ, _P]),
     "bw_ctx_set_wait_limit": (_I, [_P, _I]),
+    "bw_ctx_set_copy_chunks": (_I, [_P, _I]),
     "bw_ctx_inject_wait_fault": (_I, [_P, _I]),
     "bw_multiply_host_once": (_I, [_P, _SZ, _P, _SZ, _P, _SZ, _I,
                                    ctypes.POINTER(ctypes.c_float)]),

@@ -184,6 +184,11 @@ class Context:
     def sync(self):
         check(lib.bw_ctx_sync(self._h))
 
+    def set_copy_chunks(self, chunks):
+        """Chunks of host copies overlapped with the first and last kernels
+        (0: automatic, 1: whole copies)."""
+        check(lib.bw_ctx_set_copy_chunks(self._h, chunks))
+
     def coeffs(self, a, b):
         """Convolution coefficients after Garner, as Python ints (length n)."""
         a = _as_u32(a)

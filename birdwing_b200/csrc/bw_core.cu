@@ -509,6 +509,9 @@ extern "C" int bw_plan_get_info(const bw_plan* pl, bw_plan_info* o) {
 
 // ------------------------------------------------------------------ context
 
+// Most chunks a host copy is split into (see bw_ctx::copy_chunks).
+constexpr int kMaxCopyChunks = 16;
+
 struct bw_ctx {
     const bw_plan* plan = nullptr;
     cudaStream_t stream = nullptr;
@@ -537,6 +540,14 @@ struct bw_ctx {
     cudaEvent_t ev[8] = {};
     cudaEvent_t stage_ev[3] = {};  // ends of copy-in, kernels, copy-out (stage order)
     bool counted = false;          // included in the plan's live contexts
+    // host copies split into chunks that overlap the first and last kernels
+    // (created on first use): copy-in on in_stream, copy-out on out_stream
+    int copy_chunks = 0;           // 0: automatic, 1: whole copies on the stream
+    cudaStream_t in_stream = nullptr, out_stream = nullptr;
+    cudaEvent_t in_ev[kMaxCopyChunks] = {}, out_ev[kMaxCopyChunks] = {};
+    cudaEvent_t ready_ev = nullptr, out_done_ev = nullptr;
+    int out_pieces = 0;            // K4 launches of the last chunked product
+    size_t out_tiles_per = 0;      // carry tiles per K4 launch
     int spin_limit = 1 << 22;
     bool inject_wait_fault = false;
 };
@@ -617,6 +628,16 @@ extern "C" int bw_ctx_destroy(bw_ctx* c) {
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : c->stage_ev)
         if (ev) cudaEventDestroy(ev);
+    if (c->in_stream) cudaStreamSynchronize(c->in_stream);
+    if (c->out_stream) cudaStreamSynchronize(c->out_stream);
+    for (auto& ev : c->in_ev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : c->out_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->ready_ev) cudaEventDestroy(c->ready_ev);
+    if (c->out_done_ev) cudaEventDestroy(c->out_done_ev);
+    if (c->in_stream) cudaStreamDestroy(c->in_stream);
+    if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->h_err) cudaFreeHost(c->h_err);
     cudaFree(c->d_state);
     cudaFree(c->d_out);
@@ -629,6 +650,15 @@ extern "C" int bw_ctx_destroy(bw_ctx* c) {
 }
 
 extern "C" void* bw_ctx_stream(const bw_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int bw_ctx_set_copy_chunks(bw_ctx* c, int chunks) {
+    bw_clear_error();
+    if (!c) return bw_fail(BW_EINVAL, "NULL ctx");
+    if (chunks < 0 || chunks > kMaxCopyChunks)
+        return bw_fail(BW_EINVAL, "copy chunks %d outside 0..%d", chunks, kMaxCopyChunks);
+    c->copy_chunks = chunks;
+    return BW_OK;
+}
 
 static int read_device_errors(bw_ctx* c) {
     BW_CUDA(cudaMemcpyAsync(c->h_err, c->err, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -735,10 +765,96 @@ void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
     }
 }
 
-// Enqueue K1..K3 (the transform part) for one product.
+// Stage order of one host-pointer product (bw_stage_order): begin(i, s)
+// makes stream s wait for stage i of the plan's previous product; end(i, s)
+// records this product's stage i on s.  Off with one live context.  A
+// previous product of the same context needs no wait: every stream of a
+// product starts behind the context stream, which ends behind all of the
+// previous product's work.
+struct StageOrder {
+    bw_stage_order* so = nullptr;
+    const bw_ctx* c = nullptr;
+    bool on = false;
+    cudaError_t begin(int i, cudaStream_t s) const {
+        if (!on || !so->last[i] || so->owner[i] == c) return cudaSuccess;
+        return cudaStreamWaitEvent(s, so->last[i], 0);
+    }
+    cudaError_t end(int i, cudaStream_t s) const {
+        if (!on) return cudaSuccess;
+        const cudaError_t e = cudaEventRecord(c->stage_ev[i], s);
+        so->last[i] = c->stage_ev[i];
+        so->owner[i] = c;
+        return e;
+    }
+};
+
+// Host operands of a product whose copy-in is split into `chunks` column
+// blocks: block k holds the words of forward-column tiles
+// [k T/chunks, (k+1) T/chunks) of every row, and K1 runs over those tiles
+// as soon as the block has landed.
+struct HostIO {
+    const uint32_t* ha = nullptr;
+    const uint32_t* hb = nullptr;  // nullptr when squaring
+    int chunks = 1;
+    const StageOrder* order = nullptr;
+};
+
+// Copy words [w0, w1) of every row (row length wc words) of an operand of lx
+// words: one 2D copy over the full rows, one plain copy of the partial last
+// row's part.  Nothing at or beyond lx is read or written.
+cudaError_t copy_cols(cudaStream_t s, uint32_t* dst, const uint32_t* src, size_t lx, size_t wc,
+                      size_t w0, size_t w1) {
+    const size_t full = lx / wc;
+    cudaError_t e = cudaSuccess;
+    if (full)
+        e = cudaMemcpy2DAsync(dst + w0, wc * 4, src + w0, wc * 4, (w1 - w0) * 4, full,
+                              cudaMemcpyHostToDevice, s);
+    const size_t lo = full * wc + w0, hi = std::min(lx, full * wc + w1);
+    if (e == cudaSuccess && hi > lo)
+        e = cudaMemcpyAsync(dst + lo, src + lo, (hi - lo) * 4, cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+int ensure_copy_streams(bw_ctx* c) {
+    if (c->in_stream) return BW_OK;
+    BW_CUDA(cudaStreamCreateWithFlags(&c->in_stream, cudaStreamNonBlocking));
+    BW_CUDA(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+    for (auto& ev : c->in_ev) BW_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (auto& ev : c->out_ev) BW_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    BW_CUDA(cudaEventCreateWithFlags(&c->ready_ev, cudaEventDisableTiming));
+    BW_CUDA(cudaEventCreateWithFlags(&c->out_done_ev, cudaEventDisableTiming));
+    return BW_OK;
+}
+
+// Chunks of a host product's copies: the context's setting, else automatic:
+// whole copies while the plan's stage order is on (the products in flight
+// already hide each other's copies, and K1 and K4 in pieces cost 3-11% of
+// that pipeline's throughput), otherwise 8 from 2^23 product words and 4
+// from 2^21 (measured best; below 2^21 words the copies take less time than
+// the extra launches cost).  Capped by the forward-column tiles per operand
+// and rounded down to a power of two so that it divides them.  1 means whole
+// copies on the context stream.
+int copy_chunks_for(const bw_ctx* c, bool ordered) {
+    const bw_plan* pl = c->plan;
+    const size_t M = pl->la + pl->lb;
+    int want = c->copy_chunks;
+    if (want == 0)
+        want = ordered ? 1 : M >= ((size_t)1 << 23) ? 8 : M >= ((size_t)1 << 21) ? 4 : 1;
+    const int tiles1 = 1 << (pl->log_c + pl->log_r2 - pl->log_cb1);
+    want = std::min(std::min(want, tiles1), kMaxCopyChunks);
+    int S = 1;
+    while (S * 2 <= want) S *= 2;
+    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
+    if (S > 1 && ((tiles1 / S) << pl->log_cb1) % cpw) S = 1;
+    return S;
+}
+
+// Enqueue K1..K3 (the transform part) for one product.  With io (chunks > 1)
+// the operands' copy-in runs on the context's copy stream in column blocks
+// and K1 runs block by block behind it.
 template <class Ar, bool SPLIT16>
 int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool square,
-                      bool timing) {
+                      bool timing, const HostIO* io = nullptr) {
     using T = typename Ar::T;
     const bw_plan* pl = c->plan;
     const PlanDev<Ar>& pd = plan_dev<Ar>(pl);
@@ -753,14 +869,41 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const int CB1 = 1 << pl->log_cb1;
     const size_t smem1 = tw_bytes + (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : 4));
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
-    dim3 g1(cols_outer / CB1, 1, square ? 1 : 2);
+    const int tiles1 = cols_outer / CB1;
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
-    if (ts) {
-        k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(
-            pd, a, pl->nca, b, pl->ncb, ra, rb, zt);
+    auto k1 = [&](int tile0, int ntiles) {
+        dim3 g1(ntiles, 1, square ? 1 : 2);
+        if (ts) {
+            k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(
+                pd, a, pl->nca, b, pl->ncb, ra, rb, zt, tile0);
+        } else {
+            k_fwd_col<Ar, SPLIT16, 4, false><<<g1, kColThreads, smem1, c->stream>>>(
+                pd, a, pl->nca, b, pl->ncb, ra, rb, zt, tile0);
+        }
+    };
+    if (!io || io->chunks <= 1) {
+        k1(0, tiles1);
     } else {
-        k_fwd_col<Ar, SPLIT16, 4, false><<<g1, kColThreads, smem1, c->stream>>>(
-            pd, a, pl->nca, b, pl->ncb, ra, rb, zt);
+        // the copy stream starts where the context stream is (the previous
+        // product has read the staging buffer); block k: copy, event, K1
+        const int S = io->chunks, per = tiles1 / S, cpw = SPLIT16 ? 2 : 1;
+        const size_t wc = (size_t)cols_outer / cpw;
+        uint32_t* da = const_cast<uint32_t*>(a);
+        uint32_t* db = const_cast<uint32_t*>(b);
+        BW_CUDA(cudaEventRecord(c->ready_ev, c->stream));
+        BW_CUDA(cudaStreamWaitEvent(c->in_stream, c->ready_ev, 0));
+        BW_CUDA(io->order->begin(0, c->in_stream));
+        BW_CUDA(io->order->begin(1, c->stream));
+        for (int k = 0; k < S; ++k) {
+            const size_t w0 = ((size_t)k * per << pl->log_cb1) / cpw;
+            const size_t w1 = ((size_t)(k + 1) * per << pl->log_cb1) / cpw;
+            BW_CUDA(copy_cols(c->in_stream, da, io->ha, pl->la, wc, w0, w1));
+            if (!square) BW_CUDA(copy_cols(c->in_stream, db, io->hb, pl->lb, wc, w0, w1));
+            BW_CUDA(cudaEventRecord(c->in_ev[k], c->in_stream));
+            if (k == S - 1) BW_CUDA(io->order->end(0, c->in_stream));
+            BW_CUDA(cudaStreamWaitEvent(c->stream, c->in_ev[k], 0));
+            k1(k * per, per);
+        }
     }
     // three passes: middle column pass with the outer twiddle
     const int CB2 = 1 << pl->log_cb2;
@@ -801,7 +944,7 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
 }
 
 template <class Ar, bool SPLIT16>
-int enqueue_carry(bw_ctx* c, uint32_t* out) {
+int enqueue_carry(bw_ctx* c, uint32_t* out, int pieces = 1) {
     using T = typename Ar::T;
     const bw_plan* pl = c->plan;
     const PlanDev<Ar>& pd = plan_dev<Ar>(pl);
@@ -822,24 +965,36 @@ int enqueue_carry(bw_ctx* c, uint32_t* out) {
             pd, reinterpret_cast<const T*>(c->d_res_a), NL, c->rec_x, (uint32_t)c->ntiles,
             epoch);
     }
-    k_garner_carry<Ar, SPLIT16><<<(unsigned)c->ntiles, kCarryThreads, 0, c->stream>>>(
-        pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->cst, c->rec_x, c->rec_s,
-        epoch, c->inject_wait_fault ? epoch + (1u << 27) : epoch, c->err,
-        c->spin_limit);
+    // Tiles come from a ticket counter in launch order, so `pieces` launches
+    // in a row cover tiles [k per, (k+1) per) each; out_ev[k] marks the end of
+    // launch k, after which its words are final and can be copied out.
+    const size_t per = (c->ntiles + pieces - 1) / pieces;
+    c->out_pieces = 0;
+    c->out_tiles_per = per;
+    for (size_t t0 = 0; t0 < c->ntiles; t0 += per) {
+        const unsigned nb = (unsigned)std::min(per, c->ntiles - t0);
+        k_garner_carry<Ar, SPLIT16><<<nb, kCarryThreads, 0, c->stream>>>(
+            pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->cst, c->rec_x, c->rec_s,
+            epoch, c->inject_wait_fault ? epoch + (1u << 27) : epoch, c->err,
+            c->spin_limit);
+        if (pieces > 1) BW_CUDA(cudaEventRecord(c->out_ev[c->out_pieces], c->stream));
+        c->out_pieces++;
+    }
     BW_CUDA(cudaGetLastError());
     return BW_OK;
 }
 
 int enqueue_product(bw_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t* out,
-                    bool square, bool timing) {
+                    bool square, bool timing, const HostIO* io = nullptr) {
     const bw_plan* pl = c->plan;
+    const int pieces = io ? io->chunks : 1;
     int rc;
     if (pl->path == BW_PATH_P64) {
-        rc = enqueue_transform<Ar64, false>(c, a, b, square, timing);
-        if (!rc) rc = enqueue_carry<Ar64, false>(c, out);
+        rc = enqueue_transform<Ar64, false>(c, a, b, square, timing, io);
+        if (!rc) rc = enqueue_carry<Ar64, false>(c, out, pieces);
     } else {
-        rc = enqueue_transform<Ar32, true>(c, a, b, square, timing);
-        if (!rc) rc = enqueue_carry<Ar32, true>(c, out);
+        rc = enqueue_transform<Ar32, true>(c, a, b, square, timing, io);
+        if (!rc) rc = enqueue_carry<Ar32, true>(c, out, pieces);
     }
     return rc;
 }
@@ -936,36 +1091,55 @@ static int do_multiply(bw_ctx* c, const uint32_t* a, size_t la, const uint32_t* 
         bw_stage_order* so = pl->order;
         std::unique_lock<std::mutex> lk;
         if (so) lk = std::unique_lock<std::mutex>(so->mu);
-        const bool ordered = so && so->contexts > 1;
-        auto stage_begin = [&](int i) -> cudaError_t {
-            if (!ordered || !so->last[i] || so->owner[i] == c) return cudaSuccess;
-            return cudaStreamWaitEvent(c->stream, so->last[i], 0);
-        };
-        auto stage_end = [&](int i) -> cudaError_t {
-            if (!ordered) return cudaSuccess;
-            const cudaError_t e = cudaEventRecord(c->stage_ev[i], c->stream);
-            so->last[i] = c->stage_ev[i];
-            so->owner[i] = c;
-            return e;
-        };
-        BW_CUDA(stage_begin(0));
-        BW_CUDA(cudaMemcpyAsync(c->d_in, a, la * 4, cudaMemcpyHostToDevice, c->stream));
-        const uint32_t* db = c->d_in;
-        if (!sq) {
-            BW_CUDA(cudaMemcpyAsync(c->d_in + la, b, lb * 4, cudaMemcpyHostToDevice, c->stream));
-            db = c->d_in + la;
+        StageOrder order;
+        order.so = so;
+        order.c = c;
+        order.on = so && so->contexts > 1;
+        const uint32_t* db = sq ? c->d_in : c->d_in + la;
+        // large products without stage times: copies in chunks that overlap
+        // K1 (copy-in by column blocks) and K4 (copy-out by word ranges)
+        const int chunks = timing ? 1 : copy_chunks_for(c, order.on);
+        if (chunks > 1) {
+            rc = ensure_copy_streams(c);
+            if (rc) return rc;
+            HostIO io;
+            io.ha = a;
+            io.hb = sq ? nullptr : b;
+            io.chunks = chunks;
+            io.order = &order;
+            rc = enqueue_product(c, c->d_in, db, c->d_out, sq, false, &io);
+            if (rc) return rc;
+            BW_CUDA(order.end(1, c->stream));
+            BW_CUDA(order.begin(2, c->out_stream));
+            const size_t step = c->out_tiles_per * kCarryTileWords;
+            for (int k = 0; k < c->out_pieces; ++k) {
+                BW_CUDA(cudaStreamWaitEvent(c->out_stream, c->out_ev[k], 0));
+                const size_t lo = (size_t)k * step, hi = std::min(M, lo + step);
+                if (hi > lo)
+                    BW_CUDA(cudaMemcpyAsync(out + lo, c->d_out + lo, (hi - lo) * 4,
+                                            cudaMemcpyDeviceToHost, c->out_stream));
+            }
+            BW_CUDA(order.end(2, c->out_stream));
+            BW_CUDA(cudaEventRecord(c->out_done_ev, c->out_stream));
+            BW_CUDA(cudaStreamWaitEvent(c->stream, c->out_done_ev, 0));
+        } else {
+            BW_CUDA(order.begin(0, c->stream));
+            BW_CUDA(cudaMemcpyAsync(c->d_in, a, la * 4, cudaMemcpyHostToDevice, c->stream));
+            if (!sq)
+                BW_CUDA(cudaMemcpyAsync(c->d_in + la, b, lb * 4, cudaMemcpyHostToDevice,
+                                        c->stream));
+            BW_CUDA(order.end(0, c->stream));
+            BW_CUDA(order.begin(1, c->stream));
+            if (timing) cudaEventRecord(c->ev[1], c->stream);
+            rc = enqueue_product(c, c->d_in, db, c->d_out, sq, timing);
+            if (rc) return rc;
+            if (timing) cudaEventRecord(c->ev[5], c->stream);
+            BW_CUDA(order.end(1, c->stream));
+            BW_CUDA(order.begin(2, c->stream));
+            BW_CUDA(cudaMemcpyAsync(out, c->d_out, M * 4, cudaMemcpyDeviceToHost, c->stream));
+            BW_CUDA(order.end(2, c->stream));
+            if (timing) cudaEventRecord(c->ev[6], c->stream);
         }
-        BW_CUDA(stage_end(0));
-        BW_CUDA(stage_begin(1));
-        if (timing) cudaEventRecord(c->ev[1], c->stream);
-        rc = enqueue_product(c, c->d_in, db, c->d_out, sq, timing);
-        if (rc) return rc;
-        if (timing) cudaEventRecord(c->ev[5], c->stream);
-        BW_CUDA(stage_end(1));
-        BW_CUDA(stage_begin(2));
-        BW_CUDA(cudaMemcpyAsync(out, c->d_out, M * 4, cudaMemcpyDeviceToHost, c->stream));
-        BW_CUDA(stage_end(2));
-        if (timing) cudaEventRecord(c->ev[6], c->stream);
         if (lk.owns_lock()) lk.unlock();
         if (flags & BW_PTR_HOST_ASYNC) return BW_OK;  // bw_ctx_sync reports errors
         rc = read_device_errors(c);

@@ -310,7 +310,9 @@ __device__ __forceinline__ void stage_table(Tw<T>* dst, const Tw<T>* src, int lo
 
 // ------------------------------------------------------------------ K1
 // Forward column pass for one operand (blockIdx.z) and one tile of CB
-// columns (blockIdx.x); loops over the K primes reusing the loaded
+// columns (tile0 + blockIdx.x: a launch may cover a range of tiles, so that
+// the pass runs behind a copy-in split by columns); loops over the K primes
+// reusing the loaded
 // coefficients.  ncoef = number of coefficients of the operand; the column
 // tail beyond it is the virtual zero pad.  zt_mask bit z says operand z has
 // all coefficients in the top half of the rows (rows >= R/2 are zero).
@@ -393,12 +395,12 @@ template <class Ar, bool SPLIT16, int RLOG, bool TS>
 __global__ void __launch_bounds__(kColThreads)
 k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
           const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
-          typename Ar::T* res_b, unsigned zt_mask) {
+          typename Ar::T* res_b, unsigned zt_mask, int tile0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int op = blockIdx.z;
     fwd_col_body<Ar, SPLIT16, RLOG, TS>(P, op ? limbs_b : limbs_a, op ? ncoef_b : ncoef_a,
-                                        op ? res_b : res_a, (zt_mask >> op) & 1u, blockIdx.x,
-                                        smem_raw);
+                                        op ? res_b : res_a, (zt_mask >> op) & 1u,
+                                        tile0 + (int)blockIdx.x, smem_raw);
 }
 
 // batched: blockIdx.z = 2 * product + operand

@@ -177,6 +177,21 @@ int bw_plan_get_info(const bw_plan* plan, bw_plan_info* out);
  * issued on the given cudaStream_t. */
 int bw_ctx_create(bw_ctx** out, const bw_plan* plan, void* stream);
 int bw_ctx_destroy(bw_ctx* ctx);
+
+/* Host-pointer products (BW_PTR_HOST, BW_PTR_HOST_ASYNC) of large plans split
+ * their copies into chunks that overlap the kernels at either end: the
+ * copy-in goes in column blocks, and the first transform pass runs on each
+ * block as soon as it has landed; the copy-out goes in word ranges, each
+ * as soon as the carry pass has finished it.  The copies run on two more
+ * streams of the context, and the context stream waits for them.
+ * chunks = 0: automatic: whole copies while the plan has several live
+ * contexts (their products already overlap one another's copies), else 8
+ * from 2^23 product words, 4 from 2^21, 1 below; 1: whole copies on the
+ * context stream; 2..16: that many (rounded down to a power of two and
+ * capped by the plan's column tiles).  Calls with timing use whole
+ * copies, so that the stage times stay separate.  Reference: the ingress
+ * and egress of execute_ntt_multiply, src/gpu_ntt.cu:468-473,932-933. */
+int bw_ctx_set_copy_chunks(bw_ctx* ctx, int chunks);
 /* The cudaStream_t the context issues work on. */
 void* bw_ctx_stream(const bw_ctx* ctx);
 /* Wait for the context's stream and report device-side errors raised by

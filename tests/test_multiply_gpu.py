@@ -442,3 +442,73 @@ def test_automatic_path_choice():
                          (1 << 22, (1 << 22) + 1, 64), (1 << 23, 1 << 23, 64)]:
         with bw.Plan(la, lb) as p:
             assert p.info["path"] == want, (la, lb, p.info["path"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path,K", [(64, 2), (32, 3), (32, 2)])
+def test_chunked_host_copies(path, K):
+    """Copy-in by column blocks under K1 and copy-out by word ranges under K4,
+    for every chunk count: exact against GMP for ragged sizes (partial last
+    rows, an operand shorter than one row, unbalanced operands), squarings,
+    the three-pass schedule, pageable and pinned buffers."""
+    import torch
+    rng = np.random.default_rng(41 + path + K)
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    cases = [(300001, 299999, 0), (262144, 262144, 0), (500000, 7, 0), (123457, 65536, 0),
+             (40001, 39999, bw._lib.BW_PLAN_THREE_PASS)]
+    for la, lb, flags in cases:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = gmp_ref.mul(a, b)
+        pa, pb = pinned(a), pinned(b)
+        with bw.Plan(la, lb, path, K, flags=flags) as p, bw.Context(p) as c:
+            for chunks in (1, 2, 4, 8, 16):
+                c.set_copy_chunks(chunks)
+                assert (c.multiply(a, b) == want).all(), (la, lb, flags, chunks)
+                out = pinned(np.zeros(la + lb, dtype=np.uint32))
+                assert (c.multiply(pa, pb, out=out) == want).all(), (la, lb, flags, chunks)
+            c.set_copy_chunks(0)
+            assert (c.multiply(a, b) == want).all()
+        if la == lb or flags:
+            with bw.Plan(la, la, path, K, flags=flags) as p, bw.Context(p) as c:
+                for chunks in (1, 4, 16):
+                    c.set_copy_chunks(chunks)
+                    assert (c.square(a) == gmp_ref.mul(a, a)).all(), (la, flags, chunks)
+    with bw.Plan(1000, 1000, path, K) as p, bw.Context(p) as c:
+        with pytest.raises(bw.BwError):
+            c.set_copy_chunks(17)
+        with pytest.raises(bw.BwError):
+            c.set_copy_chunks(-1)
+
+
+@pytest.mark.gpu
+def test_chunked_copies_in_the_ordered_ring():
+    """Chunked copies on three contexts used in turn (stage order), with a
+    context reconfigured to whole copies in the middle of the stream."""
+    import torch
+    rng = np.random.default_rng(43)
+    la, lb = 1 << 20, (1 << 20) + 3
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    pairs = [(rand_words(la, rng), rand_words(lb, rng)) for _ in range(4)]
+    ins = [(pinned(a), pinned(b)) for a, b in pairs]
+    outs = [pinned(np.zeros(la + lb, dtype=np.uint32)) for _ in range(9)]
+    with bw.Plan(la, lb, 64, 2) as p:
+        ctxs = [bw.Context(p) for _ in range(3)]
+        for i in range(9):
+            c = ctxs[i % 3]
+            if i >= 3:
+                c.sync()
+            if i == 4:
+                c.set_copy_chunks(1)
+            c.multiply_async(ins[i % 4][0], ins[i % 4][1], outs[i])
+        for c in ctxs:
+            c.sync()
+        for c in ctxs:
+            c.close()
+    for i in range(9):
+        assert (outs[i] == gmp_ref.mul(*pairs[i % 4])).all(), i
