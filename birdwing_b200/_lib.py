@@ -130,6 +130,7 @@ SIGNATURES = {
     "bw_ctx_inject_wait_fault": (_I, [_P, _I]),
     "bw_multiply_host_once": (_I, [_P, _SZ, _P, _SZ, _P, _SZ, _I,
                                    ctypes.POINTER(ctypes.c_float)]),
+    "bw_host_once_cache_limit": (_I, [_SZ]),
     "bw_batch_create": (_I, [ctypes.POINTER(_P), _P, _U]),
     "bw_batch_destroy": (_I, [_P]),
     "bw_batch_clear": (_I, [_P]),

@@ -23,7 +23,7 @@ from ._lib import BwError, check, lib
 __all__ = [
     "Plan", "Context", "host_multiply_merge", "host_multiply_merge_native", "multiply",
     "square", "limits", "size_supported", "int_to_limbs", "limbs_to_int", "BwError", "Batch",
-    "tune_table", "set_tune_entry", "load_tune_table", "Server",
+    "tune_table", "set_tune_entry", "load_tune_table", "Server", "host_once_cache_limit",
 ]
 
 
@@ -207,7 +207,7 @@ class Context:
 
 
 def multiply(a, b, path=L.BW_PATH_AUTO):
-    """One-shot product of two uint32 arrays (plan, context, multiply, teardown)."""
+    """One-shot product of two uint32 arrays (plan and context cached per size)."""
     a = _as_u32(a)
     b = _as_u32(b)
     out = np.empty(a.size + b.size, dtype=np.uint32)
@@ -215,6 +215,12 @@ def multiply(a, b, path=L.BW_PATH_AUTO):
     check(lib.bw_multiply_host_once(_ptr(a), a.size, _ptr(b), b.size, _ptr(out), out.size, path,
                                     ctypes.byref(ms)))
     return out
+
+
+def host_once_cache_limit(nbytes):
+    """Device memory kept by the one-shot calls' plan/context cache
+    (``multiply``, ``host_multiply_merge``); 0 frees it and turns it off."""
+    check(lib.bw_host_once_cache_limit(int(nbytes)))
 
 
 def square(a, path=L.BW_PATH_AUTO):

@@ -1252,18 +1252,108 @@ extern "C" int bw_size_supported(int path, int num_primes, size_t la, size_t lb)
     return bw_check_size(path, K, la, lb, nullptr);
 }
 
+// Plans and contexts of recent one-shot sizes.  The reference builds and
+// uploads its tables and allocates its context on every host_multiply_merge
+// call (src/host_multiply.cpp:27-86); here a repeated size reuses them.  An
+// entry in use by one thread is skipped by the others (they build their own,
+// which then competes for the slot).  Least recently used entries go first
+// when a new one would exceed the device-memory limit.  Entries are never
+// freed at process exit (the CUDA runtime may already be gone by then).
+namespace {
+struct OnceEntry {
+    int device = 0, path = 0;
+    size_t la = 0, lb = 0, bytes = 0;
+    bw_plan* pl = nullptr;
+    bw_ctx* cx = nullptr;
+    uint64_t last_use = 0;
+    bool busy = false;
+};
+std::mutex g_once_mu;
+std::vector<OnceEntry>* g_once = new std::vector<OnceEntry>();
+size_t g_once_limit = (size_t)4 << 30;
+uint64_t g_once_clock = 0;
+
+// Frees idle entries, least recently used first, until `need` more bytes fit
+// under the limit.  Called with g_once_mu held.
+void once_evict(size_t need) {
+    for (;;) {
+        size_t used = 0;
+        for (const auto& e : *g_once) used += e.bytes;
+        if (used + need <= g_once_limit) return;
+        int victim = -1;
+        for (int i = 0; i < (int)g_once->size(); ++i)
+            if (!(*g_once)[i].busy &&
+                (victim < 0 || (*g_once)[i].last_use < (*g_once)[victim].last_use))
+                victim = i;
+        if (victim < 0) return;
+        bw_ctx_destroy((*g_once)[victim].cx);
+        bw_plan_destroy((*g_once)[victim].pl);
+        g_once->erase(g_once->begin() + victim);
+    }
+}
+}  // namespace
+
+extern "C" int bw_host_once_cache_limit(size_t bytes) {
+    bw_clear_error();
+    std::lock_guard<std::mutex> lk(g_once_mu);
+    g_once_limit = bytes;
+    once_evict(0);
+    return BW_OK;
+}
+
 extern "C" int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
                                      uint32_t* c, size_t lc, int path, float* elapsed_ms) {
     const auto t0 = std::chrono::high_resolution_clock::now();
-    bw_plan* pl = nullptr;
-    int rc = bw_plan_create(&pl, path, la, lb, 0, 0);
-    if (rc) return rc;
-    bw_ctx* cx = nullptr;
-    rc = bw_ctx_create(&cx, pl, nullptr);
-    if (!rc) rc = bw_multiply(cx, a, la, b, lb, c, lc, BW_PTR_HOST, nullptr);
-    std::string err = rc ? g_last_error : std::string();
-    bw_ctx_destroy(cx);
-    bw_plan_destroy(pl);
+    int device = 0;
+    cudaGetDevice(&device);
+    bool hit = false;  // got is a copy of a cache entry marked busy
+    OnceEntry got;
+    {
+        std::lock_guard<std::mutex> lk(g_once_mu);
+        for (auto& e : *g_once)
+            if (!e.busy && e.device == device && e.path == path && e.la == la && e.lb == lb) {
+                e.busy = true;
+                hit = true;
+                got = e;
+                break;
+            }
+    }
+    int rc = BW_OK;
+    if (!hit) {
+        got.device = device;
+        got.path = path;
+        got.la = la;
+        got.lb = lb;
+        rc = bw_plan_create(&got.pl, path, la, lb, 0, 0);
+        if (!rc) rc = bw_ctx_create(&got.cx, got.pl, nullptr);
+        if (!rc) got.bytes = ctx_bytes(got.pl) + got.pl->table_bytes;
+    }
+    if (!rc) rc = bw_multiply(got.cx, a, la, b, lb, c, lc, BW_PTR_HOST, nullptr);
+    const std::string err = rc ? g_last_error : std::string();
+    {
+        std::lock_guard<std::mutex> lk(g_once_mu);
+        if (hit) {
+            // other calls may have moved the entries: find it by its context
+            for (auto& e : *g_once)
+                if (e.cx == got.cx) {
+                    e.busy = false;
+                    e.last_use = ++g_once_clock;
+                }
+        } else if (got.cx && got.bytes <= g_once_limit) {
+            once_evict(got.bytes);
+            size_t used = 0;
+            for (const auto& e : *g_once) used += e.bytes;
+            if (used + got.bytes <= g_once_limit) {
+                got.last_use = ++g_once_clock;
+                got.busy = false;
+                g_once->push_back(got);
+                got.cx = nullptr;
+                got.pl = nullptr;
+            }
+        }
+    }
+    if (got.cx && !hit) bw_ctx_destroy(got.cx);
+    if (got.pl && !hit) bw_plan_destroy(got.pl);
     if (rc) g_last_error = err;
     const auto t1 = std::chrono::high_resolution_clock::now();
     if (elapsed_ms) *elapsed_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();

@@ -258,11 +258,20 @@ int bw_ctx_inject_wait_fault(bw_ctx* ctx, int enable);
 int bw_garner_carry_noalloc(int path, int num_primes, const void* residues, size_t n,
                             uint32_t* out, size_t out_words, void* stream);
 
-/* One-shot convenience: plan + context + multiply + teardown, host pointers.
- * (Reference: host_multiply_merge, src/host_multiply.cpp:27-86.) */
+/* One-shot convenience: plan + context + multiply, host pointers.
+ * (Reference: host_multiply_merge, src/host_multiply.cpp:27-86, which
+ * rebuilds its tables and context on every call.)  The plan and context of a
+ * size stay cached for the next call of the same size, path and device, up
+ * to bw_host_once_cache_limit bytes of device memory (least recently used
+ * sizes are freed first; a size larger than the limit is freed after its
+ * call).  Thread-safe: concurrent calls of one size use separate contexts. */
 int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b,
                           size_t lb, uint32_t* c, size_t lc, int path,
                           float* elapsed_ms);
+
+/* Device memory the one-shot cache may hold (default 4 GiB); 0 frees every
+ * idle entry and turns the cache off. */
+int bw_host_once_cache_limit(size_t bytes);
 
 /* ---------------------------------------------------------------- batches
  * Many independent products of uneven sizes in one launch sequence.  The

@@ -512,3 +512,45 @@ def test_chunked_copies_in_the_ordered_ring():
             c.close()
     for i in range(9):
         assert (outs[i] == gmp_ref.mul(*pairs[i % 4])).all(), i
+
+
+@pytest.mark.gpu
+def test_one_shot_cache():
+    """One-shot products keep the plan and context of recent sizes: repeated,
+    interleaved and concurrent calls stay exact, a small limit evicts, and a
+    zero limit frees everything and turns the cache off."""
+    import threading
+    rng = np.random.default_rng(47)
+    sizes = [(5000, 4000), (70000, 3), (1 << 16, 1 << 16), (5000, 4000)]
+    ops = [(rand_words(la, rng), rand_words(lb, rng)) for la, lb in sizes]
+    try:
+        for _ in range(2):
+            for a, b in ops:
+                assert (bw.multiply(a, b) == gmp_ref.mul(a, b)).all()
+                c, ms = bw.host_multiply_merge(a, b)
+                assert (c == gmp_ref.mul(a, b)).all() and ms > 0
+        # one size from four threads at once
+        a, b = ops[2]
+        want = gmp_ref.mul(a, b)
+        bad = []
+
+        def work():
+            for _ in range(5):
+                if not (bw.multiply(a, b) == want).all():
+                    bad.append(1)
+
+        th = [threading.Thread(target=work) for _ in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not bad
+        # a limit below one context: every call builds and frees its own
+        bw.host_once_cache_limit(1 << 20)
+        for a, b in ops:
+            assert (bw.multiply(a, b) == gmp_ref.mul(a, b)).all()
+        bw.host_once_cache_limit(0)
+        for a, b in ops[:2]:
+            assert (bw.multiply(a, b) == gmp_ref.mul(a, b)).all()
+    finally:
+        bw.host_once_cache_limit(4 << 30)
