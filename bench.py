@@ -42,20 +42,31 @@ L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
 
 CONFIGS = {
-    # name: (words_a, words_b, path, K, square, description)
+    # name: (words_a, words_b, path, K, square, description).  K and the
+    # description's coefficients are the reference's algorithm, which the
+    # oracle and the CPU baseline run; the library's plan is made with
+    # PLAN_PRIMES (0: the library chooses) and the JSON line reports what it
+    # chose (coeff_bits, num_primes, log_n).
     "2": (1 << 23, 1 << 23, 64, 2, False,
-          "plain 2^28-bit x 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
+          "plain 2^28-bit x 2^28-bit (reference algorithm: 32-bit coefficients, n=2^24, "
+          "2 x 62-bit primes)"),
     "2sq": (1 << 23, 1 << 23, 64, 2, True,
-            "squaring 2^28-bit, 32-bit coefficients, n=2^24, 2 x 62-bit primes"),
+            "squaring 2^28-bit (reference algorithm: 32-bit coefficients, n=2^24, "
+            "2 x 62-bit primes)"),
     "1": (1 << 15, 1 << 15, 32, 3, False,
           "plain 2^20-bit x 2^20-bit, 16-bit coefficients, n=2^17, 3 x 30-bit primes"),
     "4": (1 << 28, 1 << 28, 64, 3, False,
-          "plain huge 2^33-bit x 2^33-bit (1 GiB each), 32-bit coefficients, n=2^29, "
-          "3 x 62-bit primes, three-pass schedule"),
+          "plain huge 2^33-bit x 2^33-bit, 1 GiB each (reference algorithm: 32-bit "
+          "coefficients, n=2^29, 3 x 62-bit primes), three-pass schedule"),
     # a smaller product of the same kernels for ncu captures (working set > L2)
     "prof": (1 << 21, 1 << 21, 64, 2, False,
-             "plain 2^26-bit x 2^26-bit, 32-bit coefficients, n=2^22, 2 x 62-bit primes"),
+             "plain 2^26-bit x 2^26-bit (reference algorithm: 32-bit coefficients, n=2^22, "
+             "2 x 62-bit primes)"),
 }
+# num_primes of the library's plan: 0 lets it choose (on the 64-bit path at
+# these sizes: 64-bit coefficients with three primes, half the transform
+# length of the reference's 32-bit coefficients)
+PLAN_PRIMES = {"2": 0, "2sq": 0, "4": 0, "prof": 0}
 
 # batched configurations: (products, seed, K, description)
 BATCH_CONFIGS = {
@@ -894,9 +905,11 @@ def main():
         if world > 1:
             dist.barrier()
 
-    la, lb, path, K, square, desc = CONFIGS[args.config]
+    la, lb, path, K_ref, square, desc = CONFIGS[args.config]
     a, b = operands(args.config, rank)
-    plan = bw.Plan(la, lb, path, K, log_cols=args.log_cols, flags=args.plan_flags)
+    plan = bw.Plan(la, lb, path, PLAN_PRIMES.get(args.config, K_ref), log_cols=args.log_cols,
+                   flags=args.plan_flags)
+    K = plan.info["num_primes"]
     ctx = bw.Context(plan)
     stream = torch.cuda.ExternalStream(ctx.stream)
     n = plan.N
@@ -1041,7 +1054,8 @@ def main():
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64" if path == 64 else "u32", "data": "synthetic",
             "config": {"workload": f"config {args.config}: {desc}", "words_a": la,
-                       "words_b": lb, "path": path, "num_primes": K, "log_n": plan.logN,
+                       "words_b": lb, "path": path, "num_primes": K,
+                       "coeff_bits": plan.info["coeff_bits"], "log_n": plan.logN,
                        "log_cols": plan.info["log_cols"], "plan_flags": args.plan_flags,
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{world}"},

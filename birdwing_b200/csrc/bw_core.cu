@@ -265,6 +265,8 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     g.p0m2q = (T)shoup_pre(g.p0m2, p2, bits);
     g.inv2 = (T)invmod(mulmod(p0 % p2, p1 % p2, p2), p2);
     g.inv2q = (T)shoup_pre(g.inv2, p2, bits);
+    g.p01_lo = (uint64_t)((u128)p0 * p1);
+    g.p01_hi = (uint64_t)(((u128)p0 * p1) >> 64);
     pd.K = pl->K;
     pd.log_n = pl->log_n;
     pd.log_r = pl->log_r;
@@ -316,20 +318,91 @@ int bw_check_size(int path, int K, size_t la, size_t lb, int* log_n_out) {
     return BW_OK;
 }
 
+// 64-bit path with 64-bit coefficients and three primes: ceil(l / 2)
+// coefficients per operand; every coefficient of the product is below
+// min(na, nb) 2^128, far under p0 p1 p2 (2^184.9) for any size the
+// transform reaches, and all three primes carry it (none is redundant).
+int bw_check_size_w64(size_t la, size_t lb, int* log_n_out) {
+    if (la == 0 || lb == 0) return bw_fail(BW_ESIZE, "operand limb count must be positive");
+    const size_t nca = (la + 1) / 2, ncb = (lb + 1) / 2;
+    const int log_n = std::max(4, ceil_log2(nca + ncb - 1));
+    const int max_log = bw_path_max_log_n(BW_PATH_P64, 3);
+    if (log_n > max_log)
+        return bw_fail(BW_ESIZE,
+                       "transform length 2^%d for %zu x %zu words exceeds the 64-bit path limit "
+                       "2^%d",
+                       log_n, la, lb, max_log);
+    if (log_n_out) *log_n_out = log_n;
+    return BW_OK;
+}
+
+// num_primes 0 on the 64-bit path: 64-bit coefficients with three primes
+// (3 primes x n/2 points instead of 2 x n) where they halve the transform
+// and their own transform has at least 2^19 points.  On a B200 they measured
+// faster from there (2^20-word operands: 0.245 vs 0.324 ms; 2^23: 1.93 vs
+// 2.58 ms); below, the three-prime Garner and fixed costs make them slower
+// (2^18 words: 0.124 vs 0.100 ms).  Every product that BW_PATH_AUTO moves off
+// the 32-bit path (more than 2^21 of its points) has at least 2^19 of them.
+constexpr int kW64MinLogN = 19;
+
+bool bw_w64_pays(size_t la, size_t lb) {
+    int l32 = 0, l64 = 0;
+    if (bw_check_size_w64(la, lb, &l64) != BW_OK) {
+        bw_clear_error();
+        return false;
+    }
+    if (bw_check_size(BW_PATH_P64, 2, la, lb, &l32) != BW_OK) {
+        bw_clear_error();
+        return true;
+    }
+    return l64 >= kW64MinLogN && l64 < l32;
+}
+
 // BW_PATH_AUTO: the 32-bit path while its transform has at most 2^24 points
 // (its 32-bit butterflies are about four times cheaper than the 64-bit ones,
-// which more than pays for its doubled transform length: on a B200 it
-// measured 10-30% faster from 2^14- to 2^27-bit operands), the 64-bit path
-// beyond (at 2^28 bits the two measured equal) and wherever the 32-bit path
-// cannot hold the product.
+// which more than pays for its doubled transform length against 32-bit
+// coefficients on the 64-bit path: on a B200 it measured 10-30% faster from
+// 2^14- to 2^27-bit operands, equal at 2^28), the 64-bit path beyond and
+// wherever the 32-bit path cannot hold the product.  Where the 64-bit path
+// would use 64-bit coefficients (w64_ok: single products with num_primes 0)
+// the crossover is at 2^21 points of the 32-bit path: 2^20-word operands
+// measured 0.245 ms against 0.282 ms, 2^22 words 1.00 against 1.13 ms, 2^18
+// words 0.124 against 0.091 ms.
 constexpr int kAutoP32MaxLogN = 24;
+constexpr int kAutoP32MaxLogNW64 = 21;
 
-int bw_choose_path(int K, size_t la, size_t lb) {
+int bw_choose_path(int K, size_t la, size_t lb, bool w64_ok) {
     int log_n = 0;
-    if (bw_check_size(BW_PATH_P32, K, la, lb, &log_n) == BW_OK && log_n <= kAutoP32MaxLogN)
+    const int lim = w64_ok ? kAutoP32MaxLogNW64 : kAutoP32MaxLogN;
+    if (bw_check_size(BW_PATH_P32, K, la, lb, &log_n) == BW_OK && log_n <= lim)
         return BW_PATH_P32;
     bw_clear_error();
     return BW_PATH_P64;
+}
+
+// Path, prime count and coefficient width of a single-product plan.
+static int resolve_plan(int path, int num_primes, size_t la, size_t lb, unsigned flags,
+                        int* path_out, int* K_out, bool* w64_out) {
+    int K = num_primes == 0 ? 2 : num_primes;
+    const bool force64 = (flags & BW_PLAN_COEF64) != 0;
+    if (path == BW_PATH_AUTO)
+        path = force64 ? BW_PATH_P64
+                       : bw_choose_path(K < 2 || K > 3 ? 2 : K, la, lb, num_primes == 0);
+    bool w64 = false;
+    if (force64) {
+        if (path != BW_PATH_P64)
+            return bw_fail(BW_EINVAL, "64-bit coefficients need the 64-bit path");
+        if (num_primes != 0 && num_primes != 3)
+            return bw_fail(BW_EINVAL, "64-bit coefficients need num_primes 3 (or 0)");
+        w64 = true;
+    } else if (num_primes == 0 && path == BW_PATH_P64) {
+        w64 = bw_w64_pays(la, lb);
+    }
+    if (w64) K = 3;
+    *path_out = path;
+    *K_out = K;
+    *w64_out = w64;
+    return BW_OK;
 }
 
 // Streaming multiprocessors of the current device (148 on a B200).
@@ -410,7 +483,7 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         // CTAs on an SM
         pl->tw_smem_r =
             ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
-        const size_t cbytes = path == BW_PATH_P32 ? 2 : 4;
+        const size_t cbytes = path == BW_PATH_P32 ? 2 : pl->w64 ? 8 : 4;
         const size_t tsb = pl->tw_smem_r ? ((size_t)2 * w << pl->log_r) : 0;
         auto fits1 = [&](int cb) {
             const size_t elems = (size_t)1 << (pl->log_r + cb);
@@ -448,17 +521,20 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     bw_clear_error();
     if (!out) return bw_fail(BW_EINVAL, "out is NULL");
     *out = nullptr;
-    const int K = num_primes == 0 ? 2 : num_primes;
-    if (path == BW_PATH_AUTO) path = bw_choose_path(K < 2 || K > 3 ? 2 : K, la, lb);
+    int K = 0;
+    bool w64 = false;
+    int rc = resolve_plan(path, num_primes, la, lb, flags, &path, &K, &w64);
+    if (rc) return rc;
     int log_n = 0;
-    int rc = bw_check_size(path, K, la, lb, &log_n);
+    rc = w64 ? bw_check_size_w64(la, lb, &log_n) : bw_check_size(path, K, la, lb, &log_n);
     if (rc) return rc;
     bw_plan* pl = new bw_plan();
     pl->la = la;
     pl->lb = lb;
+    pl->w64 = w64 ? 1 : 0;
     const int cpw = path == BW_PATH_P32 ? 2 : 1;
-    pl->nca = la * cpw;
-    pl->ncb = lb * cpw;
+    pl->nca = w64 ? (la + 1) / 2 : la * cpw;
+    pl->ncb = w64 ? (lb + 1) / 2 : lb * cpw;
     const size_t half = ((size_t)1 << log_n) / 2;
     pl->zt_a = pl->nca <= half;
     pl->zt_b = pl->ncb <= half;
@@ -480,11 +556,17 @@ extern "C" int bw_plan_destroy(bw_plan* pl) {
     return BW_OK;
 }
 
+// Output words the plan's n coefficients cover: n/2 (16-bit), n (32-bit) or
+// 2n (64-bit coefficients).
+static size_t coef_words(const bw_plan* pl) {
+    const size_t n = (size_t)1 << pl->log_n;
+    return pl->path == BW_PATH_P32 ? n / 2 : pl->w64 ? 2 * n : n;
+}
+
 static size_t ctx_bytes(const bw_plan* pl) {
     const size_t n = (size_t)1 << pl->log_n;
     const int w = pl->path == BW_PATH_P64 ? 8 : 4;
-    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
-    const size_t nl = std::max(n / cpw, pl->la + pl->lb);
+    const size_t nl = std::max(coef_words(pl), pl->la + pl->lb);
     const size_t ntiles = (nl + kCarryTileWords - 1) / kCarryTileWords;
     return 2 * (size_t)pl->K * n * w + (pl->la + pl->lb) * 4 * 2 + 64 + ntiles * 20;
 }
@@ -497,7 +579,7 @@ extern "C" int bw_plan_get_info(const bw_plan* pl, bw_plan_info* o) {
     o->log_n = pl->log_n;
     o->log_rows = pl->log_r;
     o->log_cols = pl->log_c;
-    o->coeff_bits = pl->path == BW_PATH_P32 ? 16 : 32;
+    o->coeff_bits = pl->path == BW_PATH_P32 ? 16 : pl->w64 ? 64 : 32;
     o->la = pl->la;
     o->lb = pl->lb;
     o->lc = pl->la + pl->lb;
@@ -564,7 +646,6 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
     };
     const size_t n = (size_t)1 << pl->log_n;
     const int w = pl->path == BW_PATH_P64 ? 8 : 4;
-    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
     const size_t res_bytes = (size_t)pl->K * n * w;
     cudaError_t e;
     if (stream) {
@@ -580,9 +661,10 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
         (e = cudaMalloc(&c->d_out, ((pl->la + pl->lb + 3) & ~(size_t)3) * 4)) != cudaSuccess)
         return fail(bw_fail(BW_ENOMEM, "context allocation (%zu bytes of residues x2): %s",
                             res_bytes, cudaGetErrorString(e)));
-    // carry tiles cover the n / cpw coefficient words and the product's words
-    // (la + lb can be n / cpw + 1 when la + lb - 1 is a power of two)
-    const size_t words = std::max(n / cpw, pl->la + pl->lb);
+    // carry tiles cover the coefficients' words and the product's words
+    // (la + lb can exceed the coefficients' words when la + lb - 1 is a
+    // power of two)
+    const size_t words = std::max(coef_words(pl), pl->la + pl->lb);
     c->ntiles = (words + kCarryTileWords - 1) / kCarryTileWords;
     c->state_bytes = 32 + c->ntiles * 16 + c->ntiles * 4;
     if ((e = cudaMalloc(&c->d_state, c->state_bytes)) != cudaSuccess)
@@ -736,6 +818,10 @@ int set_smem_attrs() {
         set((const void*)k_row<Ar, 512, 3>);
         set((const void*)k_mid_col<Ar, false>);
         set((const void*)k_mid_col<Ar, true>);
+        if constexpr (sizeof(typename Ar::T) == 8) {
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, true>);
+        }
     });
     if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
     return BW_OK;
@@ -852,7 +938,7 @@ int copy_chunks_for(const bw_ctx* c, bool ordered) {
 // Enqueue K1..K3 (the transform part) for one product.  With io (chunks > 1)
 // the operands' copy-in runs on the context's copy stream in column blocks
 // and K1 runs block by block behind it.
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, bool W64 = false>
 int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool square,
                       bool timing, const HostIO* io = nullptr) {
     using T = typename Ar::T;
@@ -867,18 +953,20 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const size_t tw_bytes = ts ? (size_t)R * sizeof(Tw<T>) : 0;
 
     const int CB1 = 1 << pl->log_cb1;
-    const size_t smem1 = tw_bytes + (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : 4));
+    const size_t smem1 = tw_bytes + (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : W64 ? 8 : 4));
+    // K1 takes coefficient counts, or word counts for 64-bit coefficients
+    const size_t in_a = W64 ? pl->la : pl->nca, in_b = W64 ? pl->lb : pl->ncb;
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
     const int tiles1 = cols_outer / CB1;
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     auto k1 = [&](int tile0, int ntiles) {
         dim3 g1(ntiles, 1, square ? 1 : 2);
         if (ts) {
-            k_fwd_col<Ar, SPLIT16, 4, true><<<g1, kColThreads, smem1, c->stream>>>(
-                pd, a, pl->nca, b, pl->ncb, ra, rb, zt, tile0);
+            k_fwd_col<Ar, SPLIT16, 4, true, W64><<<g1, kColThreads, smem1, c->stream>>>(
+                pd, a, in_a, b, in_b, ra, rb, zt, tile0);
         } else {
-            k_fwd_col<Ar, SPLIT16, 4, false><<<g1, kColThreads, smem1, c->stream>>>(
-                pd, a, pl->nca, b, pl->ncb, ra, rb, zt, tile0);
+            k_fwd_col<Ar, SPLIT16, 4, false, W64><<<g1, kColThreads, smem1, c->stream>>>(
+                pd, a, in_a, b, in_b, ra, rb, zt, tile0);
         }
     };
     if (!io || io->chunks <= 1) {
@@ -886,8 +974,11 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     } else {
         // the copy stream starts where the context stream is (the previous
         // product has read the staging buffer); block k: copy, event, K1
+        // words per row of coefficients: cols / 2 (16-bit), cols (32-bit),
+        // 2 cols (64-bit coefficients)
         const int S = io->chunks, per = tiles1 / S, cpw = SPLIT16 ? 2 : 1;
-        const size_t wc = (size_t)cols_outer / cpw;
+        const size_t wpc = W64 ? 2 : 1;
+        const size_t wc = (size_t)cols_outer * wpc / cpw;
         uint32_t* da = const_cast<uint32_t*>(a);
         uint32_t* db = const_cast<uint32_t*>(b);
         BW_CUDA(cudaEventRecord(c->ready_ev, c->stream));
@@ -895,8 +986,8 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
         BW_CUDA(io->order->begin(0, c->in_stream));
         BW_CUDA(io->order->begin(1, c->stream));
         for (int k = 0; k < S; ++k) {
-            const size_t w0 = ((size_t)k * per << pl->log_cb1) / cpw;
-            const size_t w1 = ((size_t)(k + 1) * per << pl->log_cb1) / cpw;
+            const size_t w0 = ((size_t)k * per << pl->log_cb1) * wpc / cpw;
+            const size_t w1 = ((size_t)(k + 1) * per << pl->log_cb1) * wpc / cpw;
             BW_CUDA(copy_cols(c->in_stream, da, io->ha, pl->la, wc, w0, w1));
             if (!square) BW_CUDA(copy_cols(c->in_stream, db, io->hb, pl->lb, wc, w0, w1));
             BW_CUDA(cudaEventRecord(c->in_ev[k], c->in_stream));
@@ -943,13 +1034,13 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     return BW_OK;
 }
 
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, bool W64 = false>
 int enqueue_carry(bw_ctx* c, uint32_t* out, int pieces = 1) {
     using T = typename Ar::T;
     const bw_plan* pl = c->plan;
     const PlanDev<Ar>& pd = plan_dev<Ar>(pl);
     const size_t n = (size_t)1 << pl->log_n;
-    const size_t NL = n / (SPLIT16 ? 2 : 1);
+    const size_t NL = W64 ? 2 * n : n / (SPLIT16 ? 2 : 1);
     const size_t M = pl->la + pl->lb;
     uint32_t epoch = 1;
     if (!c->capturing) {
@@ -961,7 +1052,7 @@ int enqueue_carry(bw_ctx* c, uint32_t* out, int pieces = 1) {
     }
     if (c->ntiles > 1) {
         const unsigned nb = (unsigned)((c->ntiles - 1 + 255) / 256);
-        k_carry_bounds<Ar, SPLIT16><<<nb, 256, 0, c->stream>>>(
+        k_carry_bounds<Ar, SPLIT16, W64><<<nb, 256, 0, c->stream>>>(
             pd, reinterpret_cast<const T*>(c->d_res_a), NL, c->rec_x, (uint32_t)c->ntiles,
             epoch);
     }
@@ -973,7 +1064,7 @@ int enqueue_carry(bw_ctx* c, uint32_t* out, int pieces = 1) {
     c->out_tiles_per = per;
     for (size_t t0 = 0; t0 < c->ntiles; t0 += per) {
         const unsigned nb = (unsigned)std::min(per, c->ntiles - t0);
-        k_garner_carry<Ar, SPLIT16><<<nb, kCarryThreads, 0, c->stream>>>(
+        k_garner_carry<Ar, SPLIT16, W64><<<nb, kCarryThreads, 0, c->stream>>>(
             pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->cst, c->rec_x, c->rec_s,
             epoch, c->inject_wait_fault ? epoch + (1u << 27) : epoch, c->err,
             c->spin_limit);
@@ -989,7 +1080,10 @@ int enqueue_product(bw_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t* o
     const bw_plan* pl = c->plan;
     const int pieces = io ? io->chunks : 1;
     int rc;
-    if (pl->path == BW_PATH_P64) {
+    if (pl->w64) {
+        rc = enqueue_transform<Ar64, false, true>(c, a, b, square, timing, io);
+        if (!rc) rc = enqueue_carry<Ar64, false, true>(c, out, pieces);
+    } else if (pl->path == BW_PATH_P64) {
         rc = enqueue_transform<Ar64, false>(c, a, b, square, timing, io);
         if (!rc) rc = enqueue_carry<Ar64, false>(c, out, pieces);
     } else {
@@ -1195,6 +1289,10 @@ extern "C" int bw_multiply_coeffs(bw_ctx* c, const uint32_t* a, size_t la, const
     if (!c || !a || !b || !words) return bw_fail(BW_EINVAL, "NULL argument");
     const bw_plan* pl = c->plan;
     if (la != pl->la || lb != pl->lb) return bw_fail(BW_EINVAL, "operand sizes do not match plan");
+    if (pl->w64)
+        return bw_fail(BW_EINVAL,
+                       "the coefficient dump follows the reference's 32-bit coefficients: make "
+                       "the plan with num_primes 2 or 3");
     const size_t n = (size_t)1 << pl->log_n;
     if (n_words < 3 * n) return bw_fail(BW_EINVAL, "words needs 3*n = %zu entries", 3 * n);
     uint32_t* d_words = nullptr;
@@ -1247,9 +1345,11 @@ extern "C" int bw_limits(int path, int num_primes, bw_limits_info* o) {
 
 extern "C" int bw_size_supported(int path, int num_primes, size_t la, size_t lb) {
     bw_clear_error();
-    const int K = num_primes == 0 ? 2 : num_primes;
-    if (path == BW_PATH_AUTO) path = bw_choose_path(K < 2 || K > 3 ? 2 : K, la, lb);
-    return bw_check_size(path, K, la, lb, nullptr);
+    int K = 0;
+    bool w64 = false;
+    const int rc = resolve_plan(path, num_primes, la, lb, 0, &path, &K, &w64);
+    if (rc) return rc;
+    return w64 ? bw_check_size_w64(la, lb, nullptr) : bw_check_size(path, K, la, lb, nullptr);
 }
 
 // Plans and contexts of recent one-shot sizes.  The reference builds and

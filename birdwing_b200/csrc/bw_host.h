@@ -16,5 +16,7 @@ int bw_path_max_log_n(int path, int num_primes);
 // The path's primes (three entries).
 const uint64_t* bw_path_primes(int path);
 
-// The path BW_PATH_AUTO picks for a product of la x lb words with K primes.
-int bw_choose_path(int K, size_t la, size_t lb);
+// The path BW_PATH_AUTO picks for a product of la x lb words with K primes
+// (w64_ok: the 64-bit path would use 64-bit coefficients, single products
+// with num_primes 0).
+int bw_choose_path(int K, size_t la, size_t lb, bool w64_ok = false);

@@ -30,6 +30,7 @@ struct bw_plan {
     int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)
     int log_cb2 = 0, lo_out = 0;
     int small = 0;       // single-pass plan: the whole n-point transform in one CTA
+    int w64 = 0;         // 64-bit path with 64-bit coefficients (two words each, K = 3)
     int device = 0;
     bool zt_a = false, zt_b = false;
     void* d_tables = nullptr;

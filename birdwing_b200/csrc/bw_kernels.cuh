@@ -76,6 +76,7 @@ struct GarnerDev {
     T p0m2, p0m2q;      // p0 mod p2
     T inv2, inv2q;      // (p0 p1)^-1 mod p2
     uint64_t p0;        // p0 as an integer
+    uint64_t p01_lo, p01_hi;  // p0 p1 as a 128-bit integer (64-bit coefficients)
 };
 
 template <class Ar>
@@ -316,7 +317,10 @@ __device__ __forceinline__ void stage_table(Tw<T>* dst, const Tw<T>* src, int lo
 // coefficients.  ncoef = number of coefficients of the operand; the column
 // tail beyond it is the virtual zero pad.  zt_mask bit z says operand z has
 // all coefficients in the top half of the rows (rows >= R/2 are zero).
-template <class Ar, bool SPLIT16, int RLOG, bool TS>
+// W64 (64-bit path): 64-bit coefficients, two words each; ncoef is then the
+// operand's word count (an odd count leaves the last coefficient's high word
+// zero), and each coefficient enters the transform reduced to [0, 3p).
+template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false>
 __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                                              const uint32_t* __restrict__ limbs, size_t ncoef,
                                              typename Ar::T* res, bool zt_in, int tile,
@@ -329,8 +333,10 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     const size_t n = (size_t)R * C;
     const int c0 = tile << log_cb;
     const int rows_loaded = zt ? R / 2 : R;
-    // staged coefficients: 16-bit halves (32-bit path) or 32-bit limbs
-    using CT = typename std::conditional<SPLIT16, uint16_t, uint32_t>::type;
+    // staged coefficients: 16-bit halves (32-bit path), 32-bit limbs or
+    // 64-bit limb pairs (64-bit path)
+    using CT = typename std::conditional<
+        SPLIT16, uint16_t, typename std::conditional<W64, uint64_t, uint32_t>::type>::type;
 
     Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
     T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
@@ -342,6 +348,20 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             const uint32_t val =
                 ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu : 0u;
             coef[e] = (CT)val;
+        } else if constexpr (W64) {
+            // two 4-byte copies: the operand may start at an odd word
+            uint32_t* dst = reinterpret_cast<uint32_t*>(coef + e);
+            const size_t wi = 2 * ci;
+            if (wi < ncoef) {
+                cp_async_elem(dst, limbs + wi);
+            } else {
+                dst[0] = 0;
+            }
+            if (wi + 1 < ncoef) {
+                cp_async_elem(dst + 1, limbs + wi + 1);
+            } else {
+                dst[1] = 0;
+            }
         } else {
             // 32-bit limbs land in shared memory without passing registers
             if (ci < ncoef) {
@@ -372,6 +392,12 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             auto ld = [&](int v, int idx) -> T {
                 if (first) {
                     if (zt && idx >= R / 2) return T(0);
+                    if constexpr (W64) {
+                        // 2^64 < 6.0001 p: two conditional 3p steps reach [0, 3p)
+                        T x = (T)coef[(idx << log_cb) + v];
+                        x = min(x, x - ar.p3);
+                        return min(x, x - ar.p3);
+                    }
                     return (T)coef[(idx << log_cb) + v];
                 }
                 return buf[swz<T>((idx << log_cb) + v)];
@@ -391,14 +417,14 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     }
 }
 
-template <class Ar, bool SPLIT16, int RLOG, bool TS>
+template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false>
 __global__ void __launch_bounds__(kColThreads)
 k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
           const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
           typename Ar::T* res_b, unsigned zt_mask, int tile0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int op = blockIdx.z;
-    fwd_col_body<Ar, SPLIT16, RLOG, TS>(P, op ? limbs_b : limbs_a, op ? ncoef_b : ncoef_a,
+    fwd_col_body<Ar, SPLIT16, RLOG, TS, W64>(P, op ? limbs_b : limbs_a, op ? ncoef_b : ncoef_a,
                                         op ? res_b : res_a, (zt_mask >> op) & 1u,
                                         tile0 + (int)blockIdx.x, smem_raw);
 }
@@ -849,6 +875,75 @@ __device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
     *bad_out |= bad;
 }
 
+// 64-bit coefficients (three primes): the E output words from word j0 (j0
+// even, E/2 coefficients from coefficient j0/2) and the carry-out X.  Each
+// coefficient is the full mixed-radix value c = r0 + p0 k1 + p0 p1 k2
+// (< p0 p1 p2 < 2^186; the coefficients of a product stay below
+// min(na, nb) 2^128 < 2^160, so c2 >= 2^32 flags an error).  The words are
+// the low 32 E bits of V = sum_q c_q 2^(64 q), X = V >> 32 E (< 2^96).
+// Coefficients at or beyond NL / 2 read nothing and are zero.
+template <class Ar, int E, bool NC = true>
+__device__ __forceinline__ void garner_words_w64(const PlanDev<Ar>& P,
+                                                 const typename Ar::T* __restrict__ res,
+                                                 size_t n, size_t j0, size_t NL,
+                                                 uint32_t (&l)[E], uint32_t (&X)[3],
+                                                 uint32_t* bad_out) {
+    using T = typename Ar::T;
+    static_assert(sizeof(T) == 8 && E % 4 == 0, "64-bit residues, whole 16-byte loads");
+    constexpr int Q = E / 2;
+    T r[3][Q];
+#pragma unroll
+    for (int kp = 0; kp < 3; ++kp)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) r[kp][q] = 0;
+    if (j0 < NL) {
+#pragma unroll
+        for (int kp = 0; kp < 3; ++kp) {
+            const uint4* src = reinterpret_cast<const uint4*>(res + (size_t)kp * n + j0 / 2);
+#pragma unroll
+            for (int h = 0; h < Q / 2; ++h) {
+                const uint4 v = NC ? __ldg(src + h) : src[h];
+                r[kp][2 * h] = ((uint64_t)v.y << 32) | v.x;
+                r[kp][2 * h + 1] = ((uint64_t)v.w << 32) | v.z;
+            }
+        }
+    }
+    const Ar a1 = P.pr[1].ar, a2 = P.pr[2].ar;
+    const GarnerDev<Ar>& G = P.gar;
+    uint32_t bad = 0;
+    uint64_t acc0 = 0, acc1 = 0;  // running carry (< 2^96)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const T r0 = r[0][q];
+        const T r0m1 = a1.red1(a1.shoup(r0, 1, P.pr[1].one_q));
+        const T t1 = r[1][q] >= r0m1 ? r[1][q] - r0m1 : r[1][q] + a1.p - r0m1;
+        const T k1 = a1.red1(a1.shoup(t1, G.inv1, G.inv1q));
+        const T r0m2 = a2.red1(a2.shoup(r0, 1, P.pr[2].one_q));
+        const T y = a2.red1(r0m2 + a2.red1(a2.shoup(k1, G.p0m2, G.p0m2q)));
+        const T r2 = r[2][q];
+        const T t2 = r2 >= y ? r2 - y : r2 + a2.p - y;
+        const T k2 = a2.red1(a2.shoup(t2, G.inv2, G.inv2q));
+        // c = (r0 + p0 k1) + p01_lo k2 + (p01_hi k2) 2^64
+        const unsigned __int128 lo =
+            (unsigned __int128)G.p0 * k1 + r0 + (unsigned __int128)G.p01_lo * k2;  // < 2^127
+        const unsigned __int128 hi = (lo >> 64) + (unsigned __int128)G.p01_hi * k2;
+        const uint64_t c0 = (uint64_t)lo, c1 = (uint64_t)hi, c2 = (uint64_t)(hi >> 64);
+        bad |= (uint32_t)((c2 >> 32) != 0);
+        // add c to the running carry; emit 64 bits; shift
+        const unsigned __int128 s0 = (unsigned __int128)acc0 + c0;
+        l[2 * q] = (uint32_t)s0;
+        l[2 * q + 1] = (uint32_t)((uint64_t)s0 >> 32);
+        const unsigned __int128 s1 = (unsigned __int128)acc1 + c1 + (uint64_t)(s0 >> 64);
+        acc0 = (uint64_t)s1;
+        acc1 = c2 + (uint64_t)(s1 >> 64);
+    }
+    X[0] = (uint32_t)acc0;
+    X[1] = (uint32_t)(acc0 >> 32);
+    X[2] = (uint32_t)acc1;
+    bad |= (uint32_t)((acc1 >> 32) != 0);
+    *bad_out |= bad;
+}
+
 // CTA-wide resolution of a 1-bit carry chain.  Each thread has a status
 // st: 0 kill, 1 propagate, 2 generate.  chain_prepare publishes per-warp
 // aggregates (carry out for carry-in 0 / 1) in s_w and must be followed by a
@@ -887,7 +982,7 @@ __device__ __forceinline__ uint32_t chain_mine(const ChainMasks& m, const uint32
     return (carries >> lane) & 1u;
 }
 
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, bool W64 = false>
 __device__ __forceinline__ void garner_carry_body(
     const PlanDev<Ar>& P, const typename Ar::T* __restrict__ res, uint32_t* __restrict__ out,
     size_t M, size_t NL, CarryState* cst, uint4* __restrict__ rec_x,
@@ -909,16 +1004,16 @@ __device__ __forceinline__ void garner_carry_body(
     const size_t j0 = (size_t)t * TL + (size_t)tid * E;
     const size_t n = (size_t)1 << P.log_n;
 
-    // ---- Garner: digit sums D[e] < 2^96
-    unsigned __int128 D[E];
-    uint32_t bad = 0;
-    garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
-    if (bad) atomicOr(err, 2u);
-
-    // ---- local carry: words l[0..E) and carry-out X < 2^66
+    // ---- Garner and the local carry: words l[0..E) and carry-out X < 2^96
     uint32_t l[E];
     uint32_t X[3];
-    {
+    uint32_t bad = 0;
+    if constexpr (W64) {
+        garner_words_w64<Ar, E>(P, res, n, j0, NL, l, X, &bad);
+    } else {
+        // digit sums D[e] < 2^96
+        unsigned __int128 D[E];
+        garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
         unsigned __int128 acc = 0;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -930,6 +1025,7 @@ __device__ __forceinline__ void garner_carry_body(
         X[1] = (uint32_t)(acc >> 32);
         X[2] = (uint32_t)(acc >> 64);
     }
+    if (bad) atomicOr(err, 2u);
 
     // ---- the tile's carry words: the last thread's X, published at once
     // (it depends on nothing outside the tile)
@@ -1064,7 +1160,7 @@ __device__ __forceinline__ void garner_carry_body(
 // carry-out with carry-in zero), published under `epoch` before K4 runs.
 // K4 tile t then finds tile t-1's record ready and waits only on the 1-bit
 // look-back, not on its predecessor's Garner phase.  One thread per tile.
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, bool W64 = false>
 __global__ void __launch_bounds__(256)
 k_carry_bounds(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res, size_t NL,
                uint4* __restrict__ rec_x, uint32_t ntiles, uint32_t epoch) {
@@ -1073,30 +1169,39 @@ k_carry_bounds(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res, size
     if (t + 1 >= ntiles) return;
     const size_t n = (size_t)1 << P.log_n;
     const size_t j0 = (size_t)(t + 1) * kCarryTileWords - E;
-    unsigned __int128 D[E];
+    uint32_t X[3];
     uint32_t bad = 0;  // the tile's own pass reports reconstruction errors
-    garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
-    unsigned __int128 acc = 0;
+    if constexpr (W64) {
+        uint32_t l[E];
+        garner_words_w64<Ar, E>(P, res, n, j0, NL, l, X, &bad);
+    } else {
+        unsigned __int128 D[E];
+        garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
+        unsigned __int128 acc = 0;
 #pragma unroll
-    for (int e = 0; e < E; ++e) acc = (acc + D[e]) >> 32;
+        for (int e = 0; e < E; ++e) acc = (acc + D[e]) >> 32;
+        X[0] = (uint32_t)acc;
+        X[1] = (uint32_t)(acc >> 32);
+        X[2] = (uint32_t)(acc >> 64);
+    }
     uint32_t* rx = reinterpret_cast<uint32_t*>(rec_x + t);
-    st_relaxed(rx + 0, (uint32_t)acc);
-    st_relaxed(rx + 1, (uint32_t)(acc >> 32));
-    st_relaxed(rx + 2, (uint32_t)(acc >> 64));
+    st_relaxed(rx + 0, X[0]);
+    st_relaxed(rx + 1, X[1]);
+    st_relaxed(rx + 2, X[2]);
     st_release(rx + 3, epoch);
 }
 
 // Four CTAs per SM (at most 64 registers): the tile's barriers and its
 // one-bit look-back leave warps idle, which more resident CTAs cover
 // (measured 12% faster than three).
-template <class Ar, bool SPLIT16>
+template <class Ar, bool SPLIT16, bool W64 = false>
 __global__ void __launch_bounds__(kCarryThreads, 4)
 k_garner_carry(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
                uint32_t* __restrict__ out, size_t M, size_t NL, CarryState* cst,
                uint4* __restrict__ rec_x, uint32_t* __restrict__ rec_s, uint32_t epoch,
                uint32_t wait_epoch, uint32_t* __restrict__ err, int spin_limit) {
-    garner_carry_body<Ar, SPLIT16>(P, res, out, M, NL, cst, rec_x, rec_s, epoch, wait_epoch, err,
-                                   spin_limit);
+    garner_carry_body<Ar, SPLIT16, W64>(P, res, out, M, NL, cst, rec_x, rec_s, epoch,
+                                        wait_epoch, err, spin_limit);
 }
 
 // batched: blockIdx.y = product

@@ -84,6 +84,13 @@ extern "C" {
 /* Column-pass tiles of up to 128 KiB of residues instead of 64 KiB (twice
  * the columns per CTA: longer contiguous row segments, fewer CTAs per SM). */
 #define BW_PLAN_WIDE_COLS   (1u << 19)
+/* 64-bit path with 64-bit coefficients (two words each) and three primes,
+ * all three carrying the coefficients (no redundant prime): half the
+ * transform length of 32-bit coefficients for 1.5x the primes.  num_primes 0
+ * on the 64-bit path chooses it where it halves a transform of at least 2^19
+ * points; this flag forces it (num_primes must be 0 or 3).  The reference splits operands into
+ * 32-bit coefficients only (src/zero_pad.cu:3-57); the product is the same. */
+#define BW_PLAN_COEF64      (1u << 20)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
@@ -133,7 +140,7 @@ typedef struct bw_plan_info {
     int      log_n;         /* transform length n = 2^log_n                  */
     int      log_rows;      /* 4-step split n = rows * cols                   */
     int      log_cols;
-    int      coeff_bits;    /* 16 or 32                                      */
+    int      coeff_bits;    /* 16, 32 or 64 (BW_PLAN_COEF64)                 */
     size_t   la, lb;        /* operand lengths in u32 words                  */
     size_t   lc;            /* product length in u32 words (= la + lb)       */
     size_t   plan_device_bytes;   /* twiddle + constant tables               */
@@ -163,10 +170,15 @@ int bw_limits(int path, int num_primes, bw_limits_info* out);
 int bw_size_supported(int path, int num_primes, size_t la, size_t lb);
 
 /* Build the plan (twiddle tables on the device, Garner constants) for
- * products of la x lb u32 words.  path = BW_PATH_AUTO picks the faster path
- * for the size: the 32-bit path while its transform has at most 2^24 points
- * (operands up to about 2^27 bits), the 64-bit path beyond; num_primes = 0
- * picks K = 2.  The plan is bound to the current CUDA device. */
+ * products of la x lb u32 words.  num_primes = 0 lets the library choose:
+ * with path = BW_PATH_AUTO, the 32-bit path (16-bit coefficients, K = 2)
+ * while its transform has at most 2^21 points (operands up to about 2^24
+ * bits), the 64-bit path beyond; on the 64-bit path, 64-bit coefficients
+ * with K = 3 (BW_PLAN_COEF64) where they halve the transform and it has at
+ * least 2^19 points, else 32-bit coefficients with K = 2.  num_primes 2 or
+ * 3 keeps the reference's 16- or 32-bit coefficients (and then AUTO takes
+ * the 32-bit path up to 2^24 points).  The plan is bound to the current
+ * CUDA device. */
 int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb,
                    int num_primes, unsigned flags);
 int bw_plan_destroy(bw_plan* plan);

@@ -42,15 +42,18 @@ def test_limits():
     assert bw.limits(bw.BW_PATH_P64, 3)["num_primes"] == 3
 
 
-@pytest.mark.parametrize("la,lb,path,ok", [
-    (1, 1, 64, True), (1 << 23, 1 << 23, 64, True), (1 << 28, 1 << 28, 64, True),
-    (1 << 31, 1 << 31, 64, True), (1 << 32, 1 << 32, 64, False), (1 << 15, 1 << 15, 32, True),
-    (1 << 23, 1 << 23, 32, True),    # 2^24 16-bit coefficients each -> n = 2^25
-    (1 << 24, 1 << 23, 32, False),   # n = 2^26 is beyond the 32-bit path
-    (0, 5, 64, False), (5, 0, 32, False),
+@pytest.mark.parametrize("la,lb,path,K,ok", [
+    (1, 1, 64, 0, True), (1 << 23, 1 << 23, 64, 0, True), (1 << 28, 1 << 28, 64, 0, True),
+    (1 << 31, 1 << 31, 64, 2, True), (1 << 32, 1 << 32, 64, 2, False),
+    (1 << 32, 1 << 32, 64, 0, True),    # 64-bit coefficients: n = 2^32
+    (1 << 33, 1 << 33, 64, 0, False),   # n = 2^33 > v2(p - 1) = 32
+    (1 << 15, 1 << 15, 32, 0, True),
+    (1 << 23, 1 << 23, 32, 0, True),    # 2^24 16-bit coefficients each -> n = 2^25
+    (1 << 24, 1 << 23, 32, 0, False),   # n = 2^26 is beyond the 32-bit path
+    (0, 5, 64, 0, False), (5, 0, 32, 0, False),
 ])
-def test_size_supported(la, lb, path, ok):
-    good, why = bw.size_supported(la, lb, path)
+def test_size_supported(la, lb, path, K, ok):
+    good, why = bw.size_supported(la, lb, path, K)
     assert good == ok
     if not ok:
         assert why
@@ -64,7 +67,11 @@ def test_bad_arguments_are_reported_not_fatal():
     assert bw.lib.bw_plan_create(ctypes.byref(h), 64, 0, 4, 0, 0) == _lib.BW_ESIZE
     assert bw.lib.bw_plan_create(None, 64, 4, 4, 0, 0) == _lib.BW_EINVAL
     with pytest.raises(bw.BwError) as e:
-        bw.Plan(1 << 32, 1 << 32, bw.BW_PATH_P64)   # n = 2^33 > v2(p - 1) = 32
+        bw.Plan(1 << 32, 1 << 32, bw.BW_PATH_P64, 2)   # n = 2^33 > v2(p - 1) = 32
+    assert e.value.code == _lib.BW_ESIZE
+    # 64-bit coefficients halve n: 2^33-word operands need n = 2^33
+    with pytest.raises(bw.BwError) as e:
+        bw.Plan(1 << 33, 1 << 33, bw.BW_PATH_P64)
     assert e.value.code == _lib.BW_ESIZE
 
 

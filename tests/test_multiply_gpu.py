@@ -437,11 +437,21 @@ def test_p32_longest_transform_vs_gmp():
 
 
 def test_automatic_path_choice():
-    # 32-bit path while its transform has at most 2^24 points, 64-bit beyond
-    for la, lb, want in [(1, 1, 32), (1000, 700, 32), (1 << 22, 1 << 22, 32),
-                         (1 << 22, (1 << 22) + 1, 64), (1 << 23, 1 << 23, 64)]:
+    # num_primes 0: the 32-bit path while its transform has at most 2^21
+    # points, then the 64-bit path with 64-bit coefficients
+    for la, lb, want, bits in [(1, 1, 32, 16), (1000, 700, 32, 16), (1 << 19, 1 << 19, 32, 16),
+                               (1 << 19, (1 << 19) + 1, 64, 64), (1 << 22, 1 << 22, 64, 64),
+                               (1 << 23, 1 << 23, 64, 64)]:
         with bw.Plan(la, lb) as p:
-            assert p.info["path"] == want, (la, lb, p.info["path"])
+            assert (p.info["path"], p.info["coeff_bits"]) == (want, bits), (la, lb, p.info)
+    # the 64-bit path below the 64-bit-coefficient threshold keeps 32-bit ones
+    with bw.Plan(1 << 18, 1 << 18, 64) as p:
+        assert p.info["coeff_bits"] == 32 and p.info["num_primes"] == 2
+    # explicit num_primes: the reference's coefficients, the 32-bit path up to
+    # 2^24 points
+    for la, lb, want in [(1 << 22, 1 << 22, 32), (1 << 22, (1 << 22) + 1, 64)]:
+        with bw.Plan(la, lb, bw.BW_PATH_AUTO, 2) as p:
+            assert p.info["path"] == want and p.info["coeff_bits"] in (16, 32), (la, lb)
 
 
 @pytest.mark.gpu
@@ -554,3 +564,81 @@ def test_one_shot_cache():
             assert (bw.multiply(a, b) == gmp_ref.mul(a, b)).all()
     finally:
         bw.host_once_cache_limit(4 << 30)
+
+
+COEF64 = bw._lib.BW_PLAN_COEF64
+
+
+@pytest.mark.gpu
+def test_coef64_vs_gmp():
+    """64-bit coefficients with three primes (BW_PLAN_COEF64): exact against
+    GMP over odd word counts (the last coefficient without a high word),
+    single words, unbalanced operands, power-of-two boundaries, long carry
+    chains, squarings and the three-pass schedule."""
+    rng = np.random.default_rng(53)
+    shapes = [(1, 1), (1, 2), (2, 1), (3, 3), (7, 9), (8, 8), (31, 33), (64, 64), (65, 63),
+              (1000, 1), (1, 1000), (1023, 1025), (4096, 4096), (4097, 4095), (12345, 678),
+              (1 << 16, 1 << 16), ((1 << 16) + 1, (1 << 16) - 1), (300001, 299999),
+              (1 << 19, 3), (1 << 20, 1 << 20)]
+    for la, lb in shapes:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        with bw.Plan(la, lb, 64, 0, flags=COEF64) as p, bw.Context(p) as c:
+            assert p.info["coeff_bits"] == 64 and p.info["num_primes"] == 3
+            assert (c.multiply(a, b) == gmp_ref.mul(a, b)).all(), (la, lb)
+    for m in (1, 2, 7, 2048, 2049, 1 << 15, (1 << 18) + 1):
+        ones = np.full(m, 0xFFFFFFFF, dtype=np.uint32)
+        with bw.Plan(m, m, 64, 0, flags=COEF64) as p, bw.Context(p) as c:
+            assert (c.square(ones) == gmp_ref.mul(ones, ones)).all(), m
+        b = np.zeros(m + 1, dtype=np.uint32)
+        b[0] = 1
+        b[m] = 1
+        with bw.Plan(m, m + 1, 64, 0, flags=COEF64) as p, bw.Context(p) as c:
+            assert (c.multiply(ones, b) == gmp_ref.mul(ones, b)).all(), m
+    for la, lb in [(1, 1), (9, 8), (100, 77), (1000, 1000), (4096, 3000), (5000, 1),
+                   (40001, 39999)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        flags = COEF64 | bw._lib.BW_PLAN_THREE_PASS
+        with bw.Plan(la, lb, 64, 3, flags=flags) as p, bw.Context(p) as c:
+            assert (c.multiply(a, b) == gmp_ref.mul(a, b)).all(), (la, lb)
+        with bw.Plan(la, la, 64, 3, flags=flags) as p, bw.Context(p) as c:
+            assert (c.square(a) == gmp_ref.mul(a, a)).all(), la
+
+
+@pytest.mark.gpu
+def test_coef64_copies_pointers_and_choice():
+    """64-bit coefficients through chunked host copies, device pointers with
+    graph replay, and the automatic choice (num_primes 0 on the 64-bit path);
+    explicit num_primes keeps the reference's 32-bit coefficients and the
+    coefficient dump refuses 64-bit plans."""
+    import torch
+    rng = np.random.default_rng(59)
+    la, lb = 300001, 262144
+    a, b = rand_words(la, rng), rand_words(lb, rng)
+    want = gmp_ref.mul(a, b)
+    with bw.Plan(la, lb, 64) as p, bw.Context(p) as c:
+        assert p.info["coeff_bits"] == 64
+        for chunks in (1, 2, 8, 16):
+            c.set_copy_chunks(chunks)
+            assert (c.multiply(a, b) == want).all(), chunks
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(b.view(np.int32)).cuda()
+        dc = torch.zeros(la + lb, dtype=torch.int32, device="cuda")
+        for _ in range(3):
+            c.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, dc.data_ptr(), la + lb)
+            c.sync()
+            assert (dc.cpu().numpy().view(np.uint32) == want).all()
+        # operand b at an odd word offset of a device buffer
+        buf = torch.zeros(lb + 1, dtype=torch.int32, device="cuda")
+        buf[1:] = db
+        c.multiply_device(da.data_ptr(), la, buf.data_ptr() + 4, lb, dc.data_ptr(), la + lb)
+        c.sync()
+        assert (dc.cpu().numpy().view(np.uint32) == want).all()
+        with pytest.raises(bw.BwError):
+            c.coeffs(a, b)
+    for K in (2, 3):
+        with bw.Plan(la, lb, 64, K) as p:
+            assert p.info["coeff_bits"] == 32 and p.info["num_primes"] == K
+    with pytest.raises(bw.BwError):
+        bw.Plan(100, 100, 32, 0, flags=COEF64)
+    with pytest.raises(bw.BwError):
+        bw.Plan(100, 100, 64, 2, flags=COEF64)
