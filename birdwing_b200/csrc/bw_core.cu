@@ -478,12 +478,14 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         while (log_cb > min_cb && (2u << (log_cols_outer - log_cb)) < 2u * sms) --log_cb;
         pl->log_cb = log_cb;
         // forward column pass: its tile also stages the coefficients (16-bit
-        // halves as u16 on the 32-bit path, 32-bit limbs on the 64-bit path);
-        // residues + coefficients (+ staged twiddles) within 112 KiB keep two
-        // CTAs on an SM
+        // halves as u16 on the 32-bit path, 32-bit limbs on the 64-bit path of
+        // a batch group); residues + coefficients (+ staged twiddles) within
+        // 112 KiB keep two CTAs on an SM.  A single product on the 64-bit path
+        // stages them inside the residue tile (one prime per CTA), so only
+        // the residues count there.
         pl->tw_smem_r =
             ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
-        const size_t cbytes = path == BW_PATH_P32 ? 2 : pl->w64 ? 8 : 4;
+        const size_t cbytes = path == BW_PATH_P32 ? 2 : mode == 2 ? 0 : pl->w64 ? 8 : 4;
         const size_t tsb = pl->tw_smem_r ? ((size_t)2 * w << pl->log_r) : 0;
         auto fits1 = [&](int cb) {
             const size_t elems = (size_t)1 << (pl->log_r + cb);
@@ -819,8 +821,10 @@ int set_smem_attrs() {
         set((const void*)k_mid_col<Ar, false>);
         set((const void*)k_mid_col<Ar, true>);
         if constexpr (sizeof(typename Ar::T) == 8) {
-            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true>);
-            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, false, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, false, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, true, true>);
         }
     });
     if (st != cudaSuccess) return bw_fail(BW_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(st));
@@ -953,19 +957,23 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const size_t tw_bytes = ts ? (size_t)R * sizeof(Tw<T>) : 0;
 
     const int CB1 = 1 << pl->log_cb1;
-    const size_t smem1 = tw_bytes + (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : W64 ? 8 : 4));
+    // the 64-bit path stages the coefficients inside the residue tile and
+    // runs one prime per CTA (grid.y); the 32-bit path keeps a u16 copy
+    constexpr bool PP = sizeof(T) == 8;
+    const size_t smem1 =
+        tw_bytes + (size_t)R * CB1 * (sizeof(T) + (PP ? 0 : SPLIT16 ? 2 : W64 ? 8 : 4));
     // K1 takes coefficient counts, or word counts for 64-bit coefficients
     const size_t in_a = W64 ? pl->la : pl->nca, in_b = W64 ? pl->lb : pl->ncb;
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
     const int tiles1 = cols_outer / CB1;
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     auto k1 = [&](int tile0, int ntiles) {
-        dim3 g1(ntiles, 1, square ? 1 : 2);
+        dim3 g1(ntiles, PP ? pl->K : 1, square ? 1 : 2);
         if (ts) {
-            k_fwd_col<Ar, SPLIT16, 4, true, W64><<<g1, kColThreads, smem1, c->stream>>>(
+            k_fwd_col<Ar, SPLIT16, 4, true, W64, PP><<<g1, kColThreads, smem1, c->stream>>>(
                 pd, a, in_a, b, in_b, ra, rb, zt, tile0);
         } else {
-            k_fwd_col<Ar, SPLIT16, 4, false, W64><<<g1, kColThreads, smem1, c->stream>>>(
+            k_fwd_col<Ar, SPLIT16, 4, false, W64, PP><<<g1, kColThreads, smem1, c->stream>>>(
                 pd, a, in_a, b, in_b, ra, rb, zt, tile0);
         }
     };

@@ -320,11 +320,17 @@ __device__ __forceinline__ void stage_table(Tw<T>* dst, const Tw<T>* src, int lo
 // W64 (64-bit path): 64-bit coefficients, two words each; ncoef is then the
 // operand's word count (an odd count leaves the last coefficient's high word
 // zero), and each coefficient enters the transform reduced to [0, 3p).
-template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false>
+// PP (64-bit path): the CTA transforms for one prime, kp0, and stages the
+// coefficients straight into its residue tile, where the first round runs in
+// place like the others; without PP it loops over the K primes and keeps a
+// separate copy of the coefficients, which halves the tile width its shared
+// memory allows.
+template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false, bool PP = false>
 __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                                              const uint32_t* __restrict__ limbs, size_t ncoef,
                                              typename Ar::T* res, bool zt_in, int tile,
-                                             unsigned char* smem_raw) {
+                                             unsigned char* smem_raw, int kp0 = 0) {
+    static_assert(!PP || (sizeof(typename Ar::T) == 8 && !SPLIT16), "PP: 64-bit path");
     using T = typename Ar::T;
     const bool zt = zt_in && P.log_r > 0;
     const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb1;
@@ -344,7 +350,21 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
 
     for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
         const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
-        if constexpr (SPLIT16) {
+        if constexpr (PP) {
+            // into the residue tile at the first round's (swizzled) slot
+            uint32_t* dst = reinterpret_cast<uint32_t*>(buf + swz<T>(e));
+            const size_t wi = W64 ? 2 * ci : ci;
+            if (wi < ncoef) {
+                cp_async_elem(dst, limbs + wi);
+            } else {
+                dst[0] = 0;
+            }
+            if (W64 && wi + 1 < ncoef) {
+                cp_async_elem(dst + 1, limbs + wi + 1);
+            } else {
+                dst[1] = 0;
+            }
+        } else if constexpr (SPLIT16) {
             const uint32_t val =
                 ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu : 0u;
             coef[e] = (CT)val;
@@ -374,7 +394,7 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     if constexpr (!SPLIT16) cp_async_wait();
 
     const int nr = sched_rounds<RLOG>(log_r);
-    for (int kp = 0; kp < P.K; ++kp) {
+    for (int kp = PP ? kp0 : 0; kp < (PP ? kp0 + 1 : P.K); ++kp) {
         const PrimeDev<Ar>& pr = P.pr[kp];
         const Ar ar = pr.ar;
         T* gout = res + (size_t)kp * n;
@@ -392,13 +412,13 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             auto ld = [&](int v, int idx) -> T {
                 if (first) {
                     if (zt && idx >= R / 2) return T(0);
+                    T x = PP ? buf[swz<T>((idx << log_cb) + v)] : (T)coef[(idx << log_cb) + v];
                     if constexpr (W64) {
                         // 2^64 < 6.0001 p: two conditional 3p steps reach [0, 3p)
-                        T x = (T)coef[(idx << log_cb) + v];
                         x = min(x, x - ar.p3);
-                        return min(x, x - ar.p3);
+                        x = min(x, x - ar.p3);
                     }
-                    return (T)coef[(idx << log_cb) + v];
+                    return x;
                 }
                 return buf[swz<T>((idx << log_cb) + v)];
             };
@@ -417,16 +437,18 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     }
 }
 
-template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false>
+// PP: blockIdx.y = prime (64-bit path)
+template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false, bool PP = false>
 __global__ void __launch_bounds__(kColThreads)
 k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
           const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
           typename Ar::T* res_b, unsigned zt_mask, int tile0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int op = blockIdx.z;
-    fwd_col_body<Ar, SPLIT16, RLOG, TS, W64>(P, op ? limbs_b : limbs_a, op ? ncoef_b : ncoef_a,
-                                        op ? res_b : res_a, (zt_mask >> op) & 1u,
-                                        tile0 + (int)blockIdx.x, smem_raw);
+    fwd_col_body<Ar, SPLIT16, RLOG, TS, W64, PP>(P, op ? limbs_b : limbs_a,
+                                                 op ? ncoef_b : ncoef_a, op ? res_b : res_a,
+                                                 (zt_mask >> op) & 1u, tile0 + (int)blockIdx.x,
+                                                 smem_raw, PP ? (int)blockIdx.y : 0);
 }
 
 // batched: blockIdx.z = 2 * product + operand
