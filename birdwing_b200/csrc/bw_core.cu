@@ -503,7 +503,16 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         // column stage twiddles: read through L1 by default (measured faster
         // than staging them in shared memory, which costs occupancy); staged on
         // request when they take <= 32 KiB
-        pl->rlog_row = (flags & BW_PLAN_RADIX8) ? 3 : 4;
+        // row pass rounds: radix 8 for single products on the 64-bit path with
+        // rows of at most 2^12 points (its 256-thread kernel takes 64
+        // registers, no spills, and fits three CTAs per SM; measured 3-8%
+        // faster per product from 2^20 to 2^23 words), radix 16 elsewhere
+        // (2^13-point rows take 128 KiB of shared memory: one CTA per SM)
+        const bool r8_default = mode == 2 && path == BW_PATH_P64 && pl->log_c <= 12;
+        pl->rlog_row = (flags & BW_PLAN_RADIX8)    ? 3
+                       : (flags & BW_PLAN_RADIX16) ? 4
+                       : r8_default                ? 3
+                                                   : 4;
         pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
         pl->lo_out = (log_n + 1) / 2;
     }
@@ -845,8 +854,10 @@ template <class Ar, int RLOG>
 void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
                 const typename Ar::T* rb, int sq, size_t smem, cudaStream_t s) {
     dim3 g(1u << (pl->log_r + pl->log_r2), pl->K);
-    // one thread per sub-problem of a round, 64..512 threads
-    const int want = std::min(512, std::max(64, 1 << (pl->log_c - RLOG)));
+    // one thread per sub-problem of a round, 64..512 threads (radix-8 rounds:
+    // at most 256, each thread taking several sub-problems, so that the CTA's
+    // registers leave room for more than one CTA per SM)
+    const int want = std::min(RLOG == 3 ? 256 : 512, std::max(64, 1 << (pl->log_c - RLOG)));
     switch (want) {
         case 512: k_row<Ar, 512, RLOG><<<g, 512, smem, s>>>(pd, ra, rb, sq); break;
         case 256: k_row<Ar, 256, RLOG><<<g, 256, smem, s>>>(pd, ra, rb, sq); break;

@@ -91,6 +91,9 @@ extern "C" {
  * points; this flag forces it (num_primes must be 0 or 3).  The reference splits operands into
  * 32-bit coefficients only (src/zero_pad.cu:3-57); the product is the same. */
 #define BW_PLAN_COEF64      (1u << 20)
+/* Radix-16 rounds in the row pass where radix 8 is the default (single
+ * products on the 64-bit path with rows of at most 2^12 points). */
+#define BW_PLAN_RADIX16     (1u << 21)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
