@@ -34,6 +34,7 @@ BW_PLAN_THREE_PASS = 1 << 18
 BW_PLAN_WIDE_COLS = 1 << 19
 BW_PLAN_COEF64 = 1 << 20
 BW_PLAN_RADIX16 = 1 << 21
+BW_PLAN_COL_RADIX8 = 1 << 22
 
 BW_BATCH_THREE_PRIMES = 1
 BW_BATCH_UPLOAD = 1

@@ -509,6 +509,8 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         // faster per product from 2^20 to 2^23 words), radix 16 elsewhere
         // (2^13-point rows take 128 KiB of shared memory: one CTA per SM)
         const bool r8_default = mode == 2 && path == BW_PATH_P64 && pl->log_c <= 12;
+        // column passes: radix 8 on request (single products on the 64-bit path)
+        pl->rlog_col = ((flags & BW_PLAN_COL_RADIX8) && mode == 2 && path == BW_PATH_P64) ? 3 : 4;
         pl->rlog_row = (flags & BW_PLAN_RADIX8)    ? 3
                        : (flags & BW_PLAN_RADIX16) ? 4
                        : r8_default                ? 3
@@ -830,6 +832,12 @@ int set_smem_attrs() {
         set((const void*)k_mid_col<Ar, false>);
         set((const void*)k_mid_col<Ar, true>);
         if constexpr (sizeof(typename Ar::T) == 8) {
+            set((const void*)k_fwd_col<Ar, SPLIT16, 3, true, false, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 3, false, false, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 3, true, true, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 3, false, true, true>);
+            set((const void*)k_inv_col<Ar, 3, true>);
+            set((const void*)k_inv_col<Ar, 3, false>);
             set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, false, true>);
             set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, false, true>);
             set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true, true>);
@@ -980,6 +988,19 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     auto k1 = [&](int tile0, int ntiles) {
         dim3 g1(ntiles, PP ? pl->K : 1, square ? 1 : 2);
+        if constexpr (PP) {
+            if (pl->rlog_col == 3) {
+                if (ts) {
+                    k_fwd_col<Ar, SPLIT16, 3, true, W64, PP><<<g1, kColThreads, smem1, c->stream>>>(
+                        pd, a, in_a, b, in_b, ra, rb, zt, tile0);
+                } else {
+                    k_fwd_col<Ar, SPLIT16, 3, false, W64, PP>
+                        <<<g1, kColThreads, smem1, c->stream>>>(pd, a, in_a, b, in_b, ra, rb, zt,
+                                                                tile0);
+                }
+                return;
+            }
+        }
         if (ts) {
             k_fwd_col<Ar, SPLIT16, 4, true, W64, PP><<<g1, kColThreads, smem1, c->stream>>>(
                 pd, a, in_a, b, in_b, ra, rb, zt, tile0);
@@ -1043,10 +1064,23 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     }
     const size_t smem3 = tw_bytes + (size_t)R * CB * sizeof(T);
     dim3 g3(cols_outer / CB, pl->K);
-    if (ts) {
-        k_inv_col<Ar, 4, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
-    } else {
-        k_inv_col<Ar, 4, false><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+    bool inv_done = false;
+    if constexpr (PP) {
+        if (pl->rlog_col == 3) {
+            if (ts) {
+                k_inv_col<Ar, 3, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+            } else {
+                k_inv_col<Ar, 3, false><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+            }
+            inv_done = true;
+        }
+    }
+    if (!inv_done) {
+        if (ts) {
+            k_inv_col<Ar, 4, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+        } else {
+            k_inv_col<Ar, 4, false><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
+        }
     }
     if (timing) cudaEventRecord(c->ev[4], c->stream);
     BW_CUDA(cudaGetLastError());

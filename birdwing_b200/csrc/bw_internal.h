@@ -27,6 +27,7 @@ struct bw_plan {
     int log_cb1 = 0;     // forward column pass tile width (its own shared-memory budget)
     int tw_smem_r = 0;   // column stage twiddles staged in shared memory
     int rlog_row = 4;    // radix of the row kernel's rounds (2^3 or 2^4)
+    int rlog_col = 4;    // radix of the column kernels' rounds (single products, 64-bit path)
     int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)
     int log_cb2 = 0, lo_out = 0;
     int small = 0;       // single-pass plan: the whole n-point transform in one CTA

@@ -94,6 +94,8 @@ extern "C" {
 /* Radix-16 rounds in the row pass where radix 8 is the default (single
  * products on the 64-bit path with rows of at most 2^12 points). */
 #define BW_PLAN_RADIX16     (1u << 21)
+/* Radix-8 rounds in the column passes (single products on the 64-bit path). */
+#define BW_PLAN_COL_RADIX8  (1u << 22)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):

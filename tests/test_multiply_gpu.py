@@ -642,3 +642,19 @@ def test_coef64_copies_pointers_and_choice():
         bw.Plan(100, 100, 32, 0, flags=COEF64)
     with pytest.raises(bw.BwError):
         bw.Plan(100, 100, 64, 2, flags=COEF64)
+
+
+@pytest.mark.gpu
+def test_radix_switches_exact():
+    """The round-radix tuning switches of single products on the 64-bit path
+    (radix-8 column passes, radix-16 rows) keep products exact."""
+    L = bw._lib
+    rng = np.random.default_rng(61)
+    for la, lb in [(1000, 999), (65537, 4097), (300001, 299999)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = gmp_ref.mul(a, b)
+        for K, fl in ((0, COEF64), (2, 0)):
+            for sw in (L.BW_PLAN_COL_RADIX8, L.BW_PLAN_RADIX16,
+                       L.BW_PLAN_COL_RADIX8 | L.BW_PLAN_THREE_PASS):
+                with bw.Plan(la, lb, 64, K, flags=fl | sw) as p, bw.Context(p) as c:
+                    assert (c.multiply(a, b) == want).all(), (la, lb, K, sw)
