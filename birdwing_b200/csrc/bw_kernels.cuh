@@ -437,9 +437,12 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     }
 }
 
-// PP: blockIdx.y = prime (64-bit path)
+// PP: blockIdx.y = prime (64-bit path).  Three CTAs per SM (at most 85
+// registers; the 64-bit kernels then spill 32-80 bytes to the stack): the
+// shared-memory tile allows three, and the 2^28-bit product measured K1 4%
+// faster than at two (the inverse pass measured slower with the same bound).
 template <class Ar, bool SPLIT16, int RLOG, bool TS, bool W64 = false, bool PP = false>
-__global__ void __launch_bounds__(kColThreads)
+__global__ void __launch_bounds__(kColThreads, 3)
 k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoef_a,
           const uint32_t* __restrict__ limbs_b, size_t ncoef_b, typename Ar::T* res_a,
           typename Ar::T* res_b, unsigned zt_mask, int tile0) {
