@@ -647,6 +647,7 @@ def run_open_loop(srv, pool, expect, rate, duration, seed, buffers=None):
     spare = {i: list(v) for i, v in (buffers or {}).items()}
     owner = {}                                  # ticket -> (pool index, buffer, check)
     lat, late, groups, bad, checked, done_in_window = [], [], [], 0, 0, 0
+    unpinned = 0                                # outputs without a free pinned buffer
     t0 = time.perf_counter()
 
     def take_finished():
@@ -684,7 +685,11 @@ def run_open_loop(srv, pool, expect, rate, duration, seed, buffers=None):
         i = k % len(pool)
         a, b = pool[i]
         free = spare.get(i)
-        out = free.pop() if free else np.empty(len(a) + len(b), dtype=np.uint32)
+        if free:
+            out = free.pop()
+        else:
+            out = np.empty(len(a) + len(b), dtype=np.uint32)
+            unpinned += 1
         late.append((time.perf_counter() - t0 - t_arr) * 1e3)
         owner[srv.submit(a, b, out=out)] = (i, out, k % 32 == 0)
     srv.drain()
@@ -696,7 +701,7 @@ def run_open_loop(srv, pool, expect, rate, duration, seed, buffers=None):
             "mean_ms": float(np.mean(lat)) if lat else None,
             "mean_group_size": float(np.mean(groups)) if groups else None,
             "products_per_s": len(lat) / wall, "drain_s": wall - duration,
-            "completed_in_window": done_in_window}
+            "completed_in_window": done_in_window, "unpinned_outputs": unpinned}
 
 
 def run_plain_open_loop(pool, rate, duration, seed, max_wall):
@@ -761,7 +766,11 @@ def bench_serving(args):
 
     pool = [(pinned(a), None if a is b else pinned(b)) for a, b in pool]
     pool = [(a, a if b is None else b) for a, b in pool]
-    buffers = {i: [pinned(np.zeros(len(a) + len(b), dtype=np.uint32)) for _ in range(2)]
+    # four pinned output buffers per pool entry: a request whose entry has
+    # none free gets a pageable one, which the server must stage (counted as
+    # unpinned_outputs); with two, a brief latency spike at moderate rates ran
+    # them out and the slower pageable results kept the queue growing
+    buffers = {i: [pinned(np.zeros(len(a) + len(b), dtype=np.uint32)) for _ in range(4)]
                for i, (a, b) in enumerate(pool)}
     srv = bw.Server(num_primes=K)
     srv.prewarm(21)
