@@ -287,7 +287,9 @@ int bw_multiply_host_once(const uint32_t* a, size_t la, const uint32_t* b,
                           float* elapsed_ms);
 
 /* Device memory the one-shot cache may hold (default 4 GiB); 0 frees every
- * idle entry and turns the cache off. */
+ * idle entry and turns the cache off.  The cached plans and contexts belong
+ * to the device's current CUDA context: call this with 0 before resetting
+ * the device (cudaDeviceReset). */
 int bw_host_once_cache_limit(size_t bytes);
 
 /* ---------------------------------------------------------------- batches
