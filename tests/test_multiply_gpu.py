@@ -658,3 +658,44 @@ def test_radix_switches_exact():
                        L.BW_PLAN_COL_RADIX8 | L.BW_PLAN_THREE_PASS):
                 with bw.Plan(la, lb, 64, K, flags=fl | sw) as p, bw.Context(p) as c:
                     assert (c.multiply(a, b) == want).all(), (la, lb, K, sw)
+
+
+@pytest.mark.gpu
+def test_coef64_squaring_chunks_and_ring():
+    """64-bit coefficients: squarings through every chunk count, and products
+    on three contexts of one plan used in turn (stage order, whole copies)
+    then on one context (chunked copies)."""
+    import torch
+    rng = np.random.default_rng(67)
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+
+    la = (1 << 20) + 5
+    a = rand_words(la, rng)
+    want = gmp_ref.mul(a, a)
+    with bw.Plan(la, la, 64) as p, bw.Context(p) as c:
+        assert p.info["coeff_bits"] == 64
+        for chunks in (1, 2, 4, 8, 16):
+            c.set_copy_chunks(chunks)
+            assert (c.square(a) == want).all(), chunks
+    lb = (1 << 20) - 3
+    pairs = [(rand_words(la, rng), rand_words(lb, rng)) for _ in range(3)]
+    ins = [(pinned(x), pinned(y)) for x, y in pairs]
+    outs = [pinned(np.zeros(la + lb, dtype=np.uint32)) for _ in range(7)]
+    with bw.Plan(la, lb, 64) as p:
+        ctxs = [bw.Context(p) for _ in range(3)]
+        for i in range(6):
+            c = ctxs[i % 3]
+            if i >= 3:
+                c.sync()
+            c.multiply_async(ins[i % 3][0], ins[i % 3][1], outs[i])
+        for c in ctxs:
+            c.sync()
+        for c in ctxs[1:]:
+            c.close()
+        ctxs[0].multiply_async(ins[0][0], ins[0][1], outs[6])   # alone again: chunked
+        ctxs[0].sync()
+        ctxs[0].close()
+    for i in range(7):
+        assert (outs[i] == gmp_ref.mul(*pairs[i % 3])).all(), i
