@@ -113,3 +113,25 @@ def test_measured_product_is_checked():
     assert sweep.product_ok(a, b, c)
     c[1] ^= 1
     assert not sweep.product_ok(a, b, c)
+
+
+def test_command_line_with_a_stubbed_measurement(tmp_path, monkeypatch, capsys):
+    """main(): L list parsing, sizes a pipeline cannot reach reported and
+    skipped, rows appended under one header."""
+    def fake_measure(pipeline, L_arg, warmup, iters):
+        if L_arg == 30:
+            return None
+        return sweep.make_row(pipeline, L_arg, sweep.resolve_limbs(L_arg).bit_length() + 1,
+                              warmup, [1.0] * iters, [stage(*[0.1] * 6)] * iters, {}, {})
+    monkeypatch.setattr(sweep, "measure", fake_measure)
+    path = tmp_path / "cli.csv"
+    sweep.main(["--pipeline", "64bit", "--L", "6,7,30", "--iters", "2", "--csv", str(path)])
+    sweep.main(["--pipeline", "32", "--L", "8", "--iters", "1", "--csv", str(path), "--append"])
+    out = capsys.readouterr().out
+    assert "L_arg=30: beyond" in out
+    lines = path.read_text().splitlines()
+    assert lines[0] == REFERENCE_HEADER and len(lines) == 4
+    with open(path, newline="") as f:
+        rows = list(csv.DictReader(f))
+    assert [(r["pipeline"], r["L"], r["iters"]) for r in rows] == [
+        ("64bit", "64", "2"), ("64bit", "128", "2"), ("32", "256", "1")]
