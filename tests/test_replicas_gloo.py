@@ -86,3 +86,18 @@ def test_reference_arm_line_on_rank_zero(monkeypatch):
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port"
+
+
+def test_bench_configs_split_library_and_reference_primes():
+    """Plain configurations name the reference's algorithm (path, primes) for
+    the oracle and the CPU baseline; the library's plan takes PLAN_PRIMES
+    (0: its own choice) and reports what it chose."""
+    import bench
+    assert set(bench.PLAN_PRIMES) <= set(bench.CONFIGS)
+    for name, (la, lb, path, K, square, desc) in bench.CONFIGS.items():
+        assert path in (32, 64) and K in (2, 3) and la > 0 and lb > 0
+        assert bench.PLAN_PRIMES.get(name, K) in (0, 2, 3)
+        if name in bench.PLAN_PRIMES:
+            assert "reference algorithm" in desc
+    mb = bench.model_bytes(1 << 23, 1 << 23, 1 << 23, 3, 8, False)
+    assert sum(mb.values()) == 12 * 3 * (1 << 23) * 8 + 4 * (2 << 23) * 2
