@@ -1,10 +1,11 @@
 // bw_noalloc.cu -- Garner reconstruction + carry propagation that allocates
 // no device memory (bw_garner_carry_noalloc in birdwing.h).
 //
-// Who needs it: code that must not call cudaMalloc/cudaFree.  Those calls can
-// synchronise the whole device, they are not allowed while a stream is being
-// captured into a CUDA graph, and some host programs give all device memory
-// to their own pooled allocator up front.  Such callers already own the
+// Who needs it: callers that cannot call cudaMalloc/cudaFree.  Some host
+// programs hand all device memory to their own pooled allocator up front, so a
+// library allocation fails or steals from the pool; others must not let a
+// library call synchronise the whole device (cudaFree does), for example a
+// serving loop that keeps other streams busy.  Such callers already own the
 // residue arrays and the output buffer; this entry point needs nothing else
 // from them.
 //
@@ -128,7 +129,7 @@ int run(int path, int K, const void* residues, size_t n, int log_n, uint32_t* ou
         return bw_fail(BW_ESIZE,
                        "bw_garner_carry_noalloc: %zu output words need %zu carry tiles, the "
                        "fixed scratch holds %d (at most %d words)",
-                       NL, ntiles, BW_NOALLOC_MAX_TILES, BW_NOALLOC_MAX_TILES * kCarryTileWords);
+                       words, ntiles, BW_NOALLOC_MAX_TILES, BW_NOALLOC_MAX_TILES * kCarryTileWords);
     void* base = nullptr;
     int rc = scratch_for_current_device(&base);
     if (rc) return rc;
@@ -173,6 +174,17 @@ extern "C" int bw_garner_carry_noalloc(int path, int num_primes, const void* res
     if (((uintptr_t)residues & 15u) != 0)
         return bw_fail(BW_EINVAL, "residues must be 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The call reads the device error word back and waits for the stream,
+    // which a stream under capture does not allow (either would invalidate
+    // the caller's capture): refuse such a stream before touching it.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess)
+        return bw_fail(BW_ECUDA, "cudaStreamIsCapturing: %s", cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+        return bw_fail(BW_EINVAL,
+                       "bw_garner_carry_noalloc waits for its stream to read the device error "
+                       "word; the stream is being captured");
     if (path == BW_PATH_P64) return run<Ar64, false>(path, K, residues, n, log_n, out, out_words, s);
     return run<Ar32, true>(path, K, residues, n, log_n, out, out_words, s);
 }

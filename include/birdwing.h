@@ -250,30 +250,46 @@ int bw_ctx_inject_wait_fault(bw_ctx* ctx, int enable);
 #define BW_NOALLOC_MAX_TILES 32768
 
 /* Garner reconstruction + carry propagation of a finished cyclic
- * convolution, for callers that must not allocate device memory: cudaMalloc
- * and cudaFree can synchronise the whole device, are not allowed while a
- * stream is being captured into a CUDA graph, and some programs hand all
- * device memory to their own pool allocator.  This call allocates nothing.
- * The caller passes residues (device memory, 16-byte aligned): num_primes
- * arrays of n fully reduced residues, array k at residues + k * n elements,
- * u64 elements for BW_PATH_P64 and u32 for BW_PATH_P32, in natural
- * coefficient order, exactly as the library's own pipeline leaves them.  It
- * writes out[0 .. min(out_words, n / c + 1)) with c = 1 (P64) or 2 (P32: two
- * 16-bit coefficients per word); word n / c, when asked for, receives the
- * final carry.  The primes are the library's, see
- * bw_plan_get_info.  n is a power of two >= 16 and n / c is at most
- * BW_NOALLOC_MAX_TILES * 2048, else BW_ESIZE.  The look-back scratch is one
- * fixed-size device array in the library (about 640 KiB on every GPU that
- * loads it, kept until exit); every call shares it and clears the part it
- * uses, so calls whose GPU work overlaps (different streams or threads)
- * race: serialise them.  The call enqueues on `stream` and waits for it to
- * report device-side errors.  The first call on a device looks the array's
- * device address up (cudaGetSymbolAddress); make that first call before any
- * stream capture.  No counterpart in the reference: there, the CRT and
- * carry stages (src/crt_gpu.cu, src/carry_prop.cu) need buffers the caller
- * allocates with cudaMalloc. */
+ * convolution, for callers that cannot allocate device memory.  Some host
+ * programs give all device memory to their own pool allocator up front, so an
+ * allocation inside a library fails or takes memory the pool counts on; others
+ * cannot let a library call synchronise the whole device, which cudaFree does
+ * (a serving loop that keeps other streams busy, for one).  This call
+ * allocates nothing.  The caller passes residues (device memory, 16-byte
+ * aligned): num_primes arrays of n fully reduced residues, array k at
+ * residues + k * n elements, u64 elements for BW_PATH_P64 and u32 for
+ * BW_PATH_P32, in natural coefficient order.  Accepted are the residues of
+ * 32-bit coefficients on BW_PATH_P64 and of 16-bit coefficients on
+ * BW_PATH_P32 (num_primes 2, or 3 with the third prime as a check; 0 means
+ * 2), as plans with those coefficient widths leave them; residues of 64-bit
+ * coefficients (BW_PLAN_COEF64) are not.  It writes out[0 .. min(out_words,
+ * n / c + 1)) with c = 1 (P64) or 2 (P32: two 16-bit coefficients per word);
+ * word n / c, when asked for, receives the final carry.  The primes are the
+ * library's, see bw_plan_get_info.  n is a power of two >= 16 and the words
+ * written fit BW_NOALLOC_MAX_TILES * 2048, else BW_ESIZE.  The look-back
+ * scratch is one fixed-size device array in the library (about 640 KiB on
+ * every GPU that loads it, kept until exit); every call shares it and clears
+ * the part it uses, so calls whose GPU work overlaps (different streams or
+ * threads) race: serialise them.  The call enqueues on `stream`, then reads
+ * the device error word back and waits for the stream, so a stream that is
+ * being captured is refused with BW_EINVAL before anything is enqueued.  The
+ * first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress).  No counterpart in the reference: there, the CRT
+ * and carry stages (src/crt_gpu.cu, src/carry_prop.cu) need buffers the
+ * caller allocates with cudaMalloc. */
 int bw_garner_carry_noalloc(int path, int num_primes, const void* residues, size_t n,
                             uint32_t* out, size_t out_words, void* stream);
+
+/* Integer-pipe ceiling of the transforms: runs the library's own forward and
+ * inverse butterflies of one prime path (BW_PATH_P32 or BW_PATH_P64) from
+ * registers, with no memory traffic, on ctas_per_sm 256-thread CTAs per SM
+ * of the current device, `iters` times 96 butterflies per thread.  Returns
+ * the kernel's CUDA-event time and the butterflies it did; butterflies per
+ * second divided by SMs and the SM clock is the per-SM-cycle ceiling that the
+ * "fraction of the integer floor" figures divide by.  No counterpart in the
+ * reference (its NTT is the absent GPU-NTT library). */
+int bw_butterfly_rate(int path, int iters, int ctas_per_sm, float* ms,
+                      double* butterflies);
 
 /* One-shot convenience: plan + context + multiply, host pointers.
  * (Reference: host_multiply_merge, src/host_multiply.cpp:27-86, which
