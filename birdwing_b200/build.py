@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbirdwing.so")
-SOURCES = ["bw_core.cu", "bw_noalloc.cu", "bw_batch.cu", "bw_server.cu"]
+SOURCES = ["bw_core.cu", "bw_noalloc.cu", "bw_batch.cu", "bw_server.cu", "bw_probe.cu"]
 HEADERS = ["bw_arith.cuh", "bw_kernels.cuh", "bw_host.h", "bw_internal.h"]
 
 NVCC_FLAGS = [
@@ -40,11 +40,28 @@ def _stale():
 
 
 def build(force=False, verbose=False):
-    """Compile libbirdwing.so if any source is newer than it."""
+    """Compile libbirdwing.so if any source is newer than it: each source to an
+    object in parallel (the translation units are independent), then one
+    link."""
     if not force and not _stale():
         return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(ROOT, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [_nvcc()] + compile_flags + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o",
+           LIB + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

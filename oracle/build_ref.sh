@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
-# Builds the reference's own sources and tests where they lie (read-only
-# tree at $REF, default /root/reference) into oracle/_ref/.  Checker only:
+# Builds the reference's own sources and tests where they lie into
+# oracle/_ref/.  The read-only reference tree is $REF; by default the
+# directory named "reference" beside this repository's root.  Checker only:
 # nothing in the product links these.
 #
 #   _ref/ref_<w>/      the reference's compilable code with its own tests:
@@ -18,7 +19,7 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 ROOT="$(dirname "$HERE")"
-REF="${REF:-/root/reference}"
+REF="${REF:-$(dirname "$ROOT")/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-nvcc}"
 ARCH="-gencode arch=compute_100a,code=sm_100a"
