@@ -41,32 +41,26 @@ sys.path.insert(0, ROOT)
 L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
 
-CONFIGS = {
-    # name: (words_a, words_b, path, K, square, description).  K and the
-    # description's coefficients are the reference's algorithm, which the
-    # oracle and the CPU baseline run; the library's plan is made with
-    # PLAN_PRIMES (0: the library chooses) and the JSON line reports what it
-    # chose (coeff_bits, num_primes, log_n).
-    "2": (1 << 23, 1 << 23, 64, 2, False,
-          "plain 2^28-bit x 2^28-bit (reference algorithm: 32-bit coefficients, n=2^24, "
-          "2 x 62-bit primes)"),
-    "2sq": (1 << 23, 1 << 23, 64, 2, True,
-            "squaring 2^28-bit (reference algorithm: 32-bit coefficients, n=2^24, "
-            "2 x 62-bit primes)"),
-    "1": (1 << 15, 1 << 15, 32, 3, False,
-          "plain 2^20-bit x 2^20-bit, 16-bit coefficients, n=2^17, 3 x 30-bit primes"),
-    "4": (1 << 28, 1 << 28, 64, 3, False,
-          "plain huge 2^33-bit x 2^33-bit, 1 GiB each (reference algorithm: 32-bit "
-          "coefficients, n=2^29, 3 x 62-bit primes), three-pass schedule"),
-    # a smaller product of the same kernels for ncu captures (working set > L2)
-    "prof": (1 << 21, 1 << 21, 64, 2, False,
-             "plain 2^26-bit x 2^26-bit (reference algorithm: 32-bit coefficients, n=2^22, "
-             "2 x 62-bit primes)"),
-}
-# num_primes of the library's plan: 0 lets it choose (on the 64-bit path at
-# these sizes: 64-bit coefficients with three primes, half the transform
-# length of the reference's 32-bit coefficients)
-PLAN_PRIMES = {"2": 0, "2sq": 0, "4": 0, "prof": 0}
+# Plain single-product configurations come from the table the parity tests
+# also read (birdwing_b200.workloads.PLAIN): name -> (words_a, words_b, path,
+# K, square, description) of the reference's algorithm, which the oracle, the
+# CPU baseline and --impl reference run; the library's plan is built from the
+# same table's `plan` entry (plain_plan_args) and the JSON line reports what
+# it resolved to (coeff_bits, num_primes, log_n).
+from birdwing_b200.workloads import PLAIN, algorithm_of, plain_plan_args  # noqa: E402
+
+CONFIGS = {name: (w["words_a"], w["words_b"], w["ref"][0], w["ref"][1], w["square"], w["desc"])
+           for name, w in PLAIN.items()}
+
+
+def ref_algorithm(cfg):
+    """The reference's algorithm for a plain configuration, in words."""
+    la, lb, path, K, square, _ = CONFIGS[cfg]
+    cpw = 2 if path == 32 else 1
+    log_n = max(4, ((la + (la if square else lb)) * cpw - 2).bit_length())
+    return (f"reference algorithm: {32 // cpw}-bit coefficients, n=2^{log_n}, {K} x "
+            f"{62 if path == 64 else 30}-bit primes (CPU restatement)")
+
 
 # batched configurations: (products, seed, K, description)
 BATCH_CONFIGS = {
@@ -112,14 +106,17 @@ def parse_args_list(argv):
                     help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")
     ap.add_argument("--plan-flags", type=lambda s: int(s, 0), default=0,
                     help="extra bw_plan_create flags (tuning switches)")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="plain configuration 2: skip the batched and serving sub-records")
     return ap.parse_args(argv)
 
 
 def operands(cfg, rank):
     from oracle import mt64
     la, lb, path, K, square, _ = CONFIGS[cfg]
-    a = mt64.random_words_top_fast(la, 1234 + 1000 * rank)
-    b = a if square else mt64.random_words_top_fast(lb, 5678 + 1000 * rank)
+    sa, sb = PLAIN[cfg]["seeds"]
+    a = mt64.random_words_top_fast(la, sa + 1000 * rank)
+    b = a if square else mt64.random_words_top_fast(lb, sb + 1000 * rank)
     return a, b
 
 
@@ -178,18 +175,44 @@ def job_throughput(units_per_rank, world, rank_ms):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region.  NVML (the library nvidia-smi reads) is polled every 2 ms from a
+    thread, so that even a timed region of a few tens of milliseconds holds
+    samples; `region(t0, t1)` marks the timed region (time.perf_counter
+    values) and the summary covers the samples inside it.  Without NVML,
+    nvidia-smi is sampled every 100 ms instead."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.002):
         self.gpu = gpu_index
+        self.period = period_s
+        self.samples = []           # (t, sm_mhz, sm_max_mhz, set of reasons)
+        self.window = None
         self.proc = None
+        self.nvml = None
         self.lines = []
 
     def start(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self.nvml = N
+            self.h = N.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM)
+            self.bits = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
+            self.stop_flag = False
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -200,36 +223,63 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        N = self.nvml
+        while not self.stop_flag:
+            try:
+                sm = N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM)
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((time.perf_counter(), float(sm), float(self.smax),
+                                     {k for k, bit in self.bits.items() if r & bit}))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
+            parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                sm, smax = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+            reasons = {nm for nm, v in zip(self.REASONS, parts[5:9]) if v.lower() == "active"}
+            self.samples.append((time.perf_counter(), sm, smax, reasons))
+
+    def region(self, t0, t1):
+        self.window = (t0, t1)
+
+    def stop(self):
+        if self.nvml is not None:
+            self.stop_flag = True
+            self.t.join(timeout=2)
+            source = "NVML every 2 ms"
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+            source = "nvidia-smi every 100 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sel = self.samples
+        if self.window:
+            t0, t1 = self.window
+            inside = [x for x in sel if t0 <= x[0] <= t1]
+            sel = inside or sel
+        sm = [x[1] for x in sel]
+        reasons = set().union(*[x[3] for x in sel]) if sel else set()
+        out = {"sm_mhz": statistics.median(sm) if sm else None,
+               "sm_max_mhz": max(x[2] for x in sel) if sel else None,
+               "samples": len(sel), "reasons": sorted(reasons), "source": source}
+        if self.window:
+            out["region_ms"] = 1000.0 * (self.window[1] - self.window[0])
+            out["samples_in_region"] = len([x for x in self.samples
+                                            if self.window[0] <= x[0] <= self.window[1]])
+        return out
 
 
 def residue_check(a, b, got, count=3, seed=61):
@@ -321,6 +371,7 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic", "config": {"workload": f"config {args.config}: {desc}",
+                                            "algorithm": ref_algorithm(args.config),
                                             "words_a": la, "words_b": lb, "path": path,
                                             "num_primes": K},
             "cpu_baseline": cb,
@@ -348,6 +399,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1000 * dt / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic", "config": {"workload": f"config {args.config}: {desc}",
+                                        "algorithm": ref_algorithm(args.config),
                                         "words_a": la, "words_b": lb, "path": path,
                                         "num_primes": K},
         "cpu_baseline": {"value": v, "unit": "products/s", "cores": cores, "kind": "port",
@@ -897,7 +949,95 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    bench_plain(args)
 
+
+def fixed_model(cfg):
+    """The fixed algorithmic byte model of a plain configuration (SURVEY-style
+    12*K*n*w + in + out, 9*K*n*w + in + out when squaring) evaluated on the
+    workload as the reference states it (its coefficient width, prime count
+    and prime width), whatever algorithm the library chose.  Returns (bytes,
+    K, n, w)."""
+    la, lb, path, K, square, _ = CONFIGS[cfg]
+    cpw = 2 if path == 32 else 1
+    log_n = max(4, ((la + (la if square else lb)) * cpw - 2).bit_length())
+    n, w = 1 << log_n, (8 if path == 64 else 4)
+    io = 4 * (la + (0 if square else lb)) + 4 * (la + lb)
+    return (9 if square else 12) * K * n * w + io, K, n, w
+
+
+def plan_butterflies(info, square):
+    """Butterflies of one product: T transforms (3, or 2 when squaring) of K
+    primes, each (n/2) log2 n."""
+    t = 2 if square else 3
+    return t * info["num_primes"] * (1 << (info["log_n"] - 1)) * info["log_n"]
+
+
+def butterfly_rate(path, iters=2000):
+    """Integer-pipe ceiling of the path's butterflies (bw_butterfly_rate):
+    butterflies per second with nothing else running, best of 3."""
+    import ctypes
+
+    from birdwing_b200 import _lib as L
+    best = None
+    for _ in range(3):
+        ms, bf = ctypes.c_float(), ctypes.c_double()
+        L.check(L.lib.bw_butterfly_rate(path, iters, 4, ctypes.byref(ms), ctypes.byref(bf)))
+        r = bf.value / (ms.value * 1e-3)
+        best = r if best is None else max(best, r)
+    return best
+
+
+def run_sub_bench(extra, timeout):
+    """Run this script once more as a child process (one GPU, no torchrun
+    variables) and return its JSON line, or {"error": ...}."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE", "MASTER_ADDR",
+                        "MASTER_PORT", "GROUP_RANK", "ROLE_RANK", "TORCHELASTIC_RUN_ID")}
+    cmd = [sys.executable, os.path.abspath(__file__)] + extra
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, env=env)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s", "cmd": " ".join(extra)}
+    for ln in reversed(r.stdout.strip().splitlines()):
+        if ln.startswith("{"):
+            try:
+                return json.loads(ln)
+            except ValueError:
+                break
+    return {"error": f"exit {r.returncode}: {r.stderr.strip()[-400:]}", "cmd": " ".join(extra)}
+
+
+def batched_summary(line):
+    if "error" in line:
+        return line
+    pl = line.get("plain_loop") or {}
+    return {"workload": line["config"]["workload"], "value": line["value"],
+            "unit": line["unit"], "ms_per_step": line["ms_per_step"],
+            "plain_loop_value": pl.get("value"),
+            "batched_over_plain": line.get("batched_over_plain"),
+            "e2e_value": line["e2e"]["value"], "correct_vs_gmp": line["correct_vs_gmp"],
+            "buckets": line["config"]["buckets"], "clocks": line.get("clocks"),
+            "cmd": "python bench.py --config 3 --steps 10 --warmup 3 --e2e-steps 2 "
+                   "--no-cpu-baseline"}
+
+
+def serving_summary(line):
+    if "error" in line:
+        return line
+    plain = line.get("plain_per_request") or {}
+    return {"workload": line["config"]["workload"], "value": line["value"],
+            "unit": line["unit"], "p50_ms": line["latency_ms"]["p50"],
+            "p99_ms": line["latency_ms"]["p99"], "at_rate": line["latency_ms"]["at_rate"],
+            "capacity_closed_loop": line["config"]["capacity_closed_loop"],
+            "plain_per_request": {k: plain.get(k) for k in ("rate", "products_per_s", "p50_ms",
+                                                            "p99_ms", "unserved_at_cutoff")},
+            "correct_vs_gmp": line["correct_vs_gmp"], "clocks": line.get("clocks"),
+            "cmd": "python bench.py --config 5 --duration 4 --rate-fracs 0.45 --warmup 1 "
+                   "--no-cpu-baseline"}
+
+
+def bench_plain(args):
     import torch
     import torch.distributed as dist
 
@@ -914,15 +1054,16 @@ def main():
         if world > 1:
             dist.barrier()
 
-    la, lb, path, K_ref, square, desc = CONFIGS[args.config]
-    a, b = operands(args.config, rank)
-    plan = bw.Plan(la, lb, path, PLAN_PRIMES.get(args.config, K_ref), log_cols=args.log_cols,
-                   flags=args.plan_flags)
-    K = plan.info["num_primes"]
+    cfg = args.config
+    la, lb, _, _, square, desc = CONFIGS[cfg]
+    _, _, ppath, pk, pflags = plain_plan_args(cfg)
+    a, b = operands(cfg, rank)
+    plan = bw.Plan(la, lb, ppath, pk, log_cols=args.log_cols, flags=pflags | args.plan_flags)
+    info = plan.info
+    K, n, path = info["num_primes"], plan.N, info["path"]
+    w = 8 if path == 64 else 4
     ctx = bw.Context(plan)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    n = plan.N
-    w = 8 if path == 64 else 4
 
     # inputs resident in HBM for the device-time measurement
     da = torch.from_numpy(a.view(np.int32)).cuda()
@@ -930,63 +1071,71 @@ def main():
     dc = torch.empty(la + lb, dtype=torch.int32, device="cuda")
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
 
-    def step(timing):
-        return ctx.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, dc.data_ptr(), la + lb,
-                                   timing=timing)
+    def make_step(c):
+        def step(timing):
+            return c.multiply_device(da.data_ptr(), la, db.data_ptr(), lb, dc.data_ptr(),
+                                     la + lb, timing=timing)
+        return step
 
+    def check_product():
+        got = dc.cpu().numpy().view(np.uint32)
+        if cfg in CPU_SAMPLE_WORDS:
+            return residue_check(a, b, got), "residues mod 2^64 and three random 61-bit primes"
+        from oracle import gmp_ref
+        return bool((got == gmp_ref.mul(a, b)).all()), "GMP mpz_mul"
+
+    def timed_products(c, st, steps, sampler=None):
+        """steps whole products back to back on the context stream (graph
+        replays), L2 flushed before each; returns the per-step event times."""
+        step = make_step(c)
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(steps):
+            with torch.cuda.stream(st):
+                flush.fill_(i)                       # evict L2 between steps
+                ev0[i].record(st)
+            step(False)
+            with torch.cuda.stream(st):
+                ev1[i].record(st)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.region(t0, time.perf_counter())
+        return [e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1)]
+
+    def stage_means(c, st, reps):
+        """Per-stage device times (events between the kernels, direct
+        launches), outside the timed region."""
+        step = make_step(c)
+        stage = {k: [] for k in ("fwd_ms", "mul_ms", "intt_ms", "crt_carry_ms")}
+        for i in range(reps):
+            with torch.cuda.stream(st):
+                flush.fill_(i)
+            t = step(True)
+            for k in stage:
+                stage[k].append(t[k])
+        return {k: statistics.mean(v) for k, v in stage.items()}
+
+    step = make_step(ctx)
     for _ in range(max(3, args.warmup)):
         step(False)
     ctx.sync()
     # correctness of the benchmarked product (once, outside the timed region)
-    check = "GMP mpz_mul"
-    if rank == 0:
-        got = dc.cpu().numpy().view(np.uint32)
-        if args.config in CPU_SAMPLE_WORDS:
-            check = "residues mod 2^64 and three random 61-bit primes"
-            ok = residue_check(a, b, got)
-        else:
-            from oracle import gmp_ref
-            ok = bool((got == gmp_ref.mul(a, b)).all())
-        del got
-    else:
-        ok = True
-    device_bytes = (plan.info["plan_device_bytes"] + plan.info["ctx_device_bytes"] +
+    ok, check = check_product() if rank == 0 else (True, "")
+    device_bytes = (info["plan_device_bytes"] + info["ctx_device_bytes"] +
                     4 * (la + (0 if square else lb)) + 4 * (la + lb))
 
     sampler = ClockSampler(local)
-    stage = {k: [] for k in ("fwd_ms", "mul_ms", "intt_ms", "crt_carry_ms")}
-    per_step = []
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    barrier()
-    torch.cuda.synchronize()
     sampler.start()
-    time.sleep(0.3)
-    # timed: whole products, back to back on the context stream (the library
-    # replays one CUDA graph of the pipeline), L2 flushed before each
-    for i in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(i)                       # evict L2 between steps
-            ev0[i].record(stream)
-        step(False)
-        with torch.cuda.stream(stream):
-            ev1[i].record(stream)
-    torch.cuda.synchronize()
-    # per-stage device times (events between the kernels, direct launches),
-    # outside the timed region
-    for i in range(max(3, min(args.steps, 10))):
-        with torch.cuda.stream(stream):
-            flush.fill_(i)
-        t = step(True)
-        for k in stage:
-            stage[k].append(t[k])
+    time.sleep(0.05)
+    per_step = timed_products(ctx, stream, args.steps, sampler)
+    stage = stage_means(ctx, stream, max(3, min(args.steps, 10)))
     clocks = sampler.stop()
     barrier()
     ctx.sync()
-    for i in range(args.steps):
-        per_step.append(ev0[i].elapsed_time(ev1[i]))
-    total_ms = sum(per_step)
-    total_ms = reduce_over_ranks([total_ms], ["max"])[0]
+    total_ms = reduce_over_ranks([sum(per_step)], ["max"])[0]
 
     # end to end through the C ABI with pinned host buffers
     ha = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
@@ -1038,7 +1187,7 @@ def main():
     e2e_pipe_total = reduce_over_ranks([1000 * (time.perf_counter() - t0)], ["max"])[0]
     ok_e2e = True
     if rank == 0:
-        if args.config in CPU_SAMPLE_WORDS:
+        if cfg in CPU_SAMPLE_WORDS:
             ok_e2e = all(residue_check(a, b, o_) for _, o_ in ring)
         else:
             from oracle import gmp_ref
@@ -1047,39 +1196,68 @@ def main():
     for c_, _ in ring[1:]:
         c_.close()
 
+    # the workload as the reference states it (its coefficient width and
+    # prime count), when the library's own plan differs: same operands, same
+    # timing, rank 0 of a single-GPU run
+    literal = None
+    lp = plain_plan_args(cfg, "literal")
+    if world == 1 and PLAIN[cfg]["literal"] != PLAIN[cfg]["plan"]:
+        with bw.Plan(*lp[:4], flags=lp[4]) as lplan, bw.Context(lplan) as lctx:
+            lst = torch.cuda.ExternalStream(lctx.stream)
+            lstep = make_step(lctx)
+            for _ in range(3):
+                lstep(False)
+            lctx.sync()
+            lok, _ = check_product()
+            lper = timed_products(lctx, lst, max(args.steps, 20))
+            lstage = stage_means(lctx, lst, 5)
+            lctx.sync()
+            li = lplan.info
+            literal = {"algorithm": algorithm_of(li), "coeff_bits": li["coeff_bits"],
+                       "num_primes": li["num_primes"], "log_n": li["log_n"],
+                       "ms_per_step": sum(lper) / len(lper),
+                       "value": len(lper) / (sum(lper) * 1e-3), "unit": "products/s",
+                       "stage_ms": lstage, "correct_vs_gmp": lok}
+
     if rank == 0:
         ms = total_ms / args.steps
         mb = model_bytes(la, lb, n, K, w, square)
-        means = {k: statistics.mean(v) for k, v in stage.items()}
-        dom = max(means, key=means.get)
+        dom = max(stage, key=stage.get)
         kernel_names = {"fwd_ms": "k_fwd_col", "mul_ms": "k_row", "intt_ms": "k_inv_col",
                         "crt_carry_ms": "k_garner_carry"}
         peak, peak_kind = load_peaks()
-        achieved = mb[dom] / (means[dom] * 1e-3) / 1e9
-        total_model = sum(mb.values())
+        achieved = mb[dom] / (stage[dom] * 1e-3) / 1e9
+        own_model = sum(mb.values())
+        fixed, fk, fn, fw = fixed_model(cfg)
         line = {
             "metric": "products/s", "value": job_throughput(args.steps, world, total_ms),
             "unit": "products/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64" if path == 64 else "u32", "data": "synthetic",
-            "config": {"workload": f"config {args.config}: {desc}", "words_a": la,
-                       "words_b": lb, "path": path, "num_primes": K,
-                       "coeff_bits": plan.info["coeff_bits"], "log_n": plan.logN,
-                       "log_cols": plan.info["log_cols"], "plan_flags": args.plan_flags,
+            "config": {"workload": f"config {cfg}: {desc}", "algorithm": algorithm_of(info),
+                       "words_a": la, "words_b": lb, "path": path, "num_primes": K,
+                       "coeff_bits": info["coeff_bits"], "log_n": plan.logN,
+                       "log_cols": info["log_cols"], "plan_flags": pflags | args.plan_flags,
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "correct_vs_gmp": ok,
             "correctness_check": check,
             "hbm_footprint_bytes": device_bytes,
-            "stage_ms": means,
+            "stage_ms": stage,
             "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
-                         "traffic": load_traffic(args.config, kernel_names[dom]),
-                         "algorithmic_bytes": mb[dom]},
-            "product_roofline": {"model_bytes": total_model,
-                                 "achieved": total_model / (ms * 1e-3) / 1e9, "unit": "GB/s",
-                                 "frac": total_model / (ms * 1e-3) / 1e9 / peak},
+                         "traffic": load_traffic(cfg, kernel_names[dom]),
+                         "algorithmic_bytes": mb[dom],
+                         "bytes_model": "the chosen algorithm's K*n*w per kernel"},
+            "product_roofline": {
+                "fixed_model_bytes": fixed,
+                "fixed_model": f"12*K*n*w + in + out at the workload's stated K={fk}, "
+                               f"n=2^{fn.bit_length() - 1}, w={fw}",
+                "achieved": fixed / (ms * 1e-3) / 1e9, "unit": "GB/s",
+                "frac": fixed / (ms * 1e-3) / 1e9 / peak,
+                "own_model_bytes": own_model,
+                "own_model_frac": own_model / (ms * 1e-3) / 1e9 / peak},
             "e2e": {"value": job_throughput(e2e_steps, world, e2e_pipe_total),
                     "unit": "products/s", "h2d_bytes_per_step": 4 * (la + (0 if square else lb)),
                     "d2h_bytes_per_step": 4 * (la + lb) + 4,
@@ -1091,11 +1269,33 @@ def main():
                     "blocking_pageable_value": job_throughput(min(args.e2e_steps, 3), world,
                                                               e2e_pg_total),
                     "correct_vs_gmp": ok_e2e},
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": (5 if (la + lb) > 2048 else 4) * args.steps,
             "clocks": clocks,
         }
+        if literal:
+            literal["product_roofline_frac"] = fixed / (literal["ms_per_step"] * 1e-3) / 1e9 / peak
+            line["literal_config"] = literal
+        if world == 1:
+            # integer-pipe floor: the plan's butterflies at the rate the
+            # path's butterflies reach with nothing else running
+            rate = butterfly_rate(path)
+            bfly = plan_butterflies(info, square)
+            floor_ms = bfly / rate * 1e3
+            line["int_floor"] = {"butterflies": bfly, "butterflies_per_s": rate,
+                                 "floor_ms": floor_ms, "frac": floor_ms / ms,
+                                 "how": "bw_butterfly_rate: the path's own forward and inverse "
+                                        "butterflies from registers on 4 CTAs per SM, best of 3"}
+            line["int_floor_frac"] = floor_ms / ms
         if not args.no_cpu_baseline and world == 1:   # the CPU baseline runs at N = 1 only
-            line["cpu_baseline"] = cpu_baseline(args.config)
+            line["cpu_baseline"] = cpu_baseline(cfg)
+        if cfg == "2" and world == 1 and not args.no_sub:
+            # the metric's other halves, each in a child process of its own
+            line["batched"] = batched_summary(run_sub_bench(
+                ["--config", "3", "--steps", "10", "--warmup", "3", "--e2e-steps", "2",
+                 "--no-cpu-baseline"], timeout=300))
+            line["serving"] = serving_summary(run_sub_bench(
+                ["--config", "5", "--duration", "4", "--rate-fracs", "0.45", "--warmup", "1",
+                 "--no-cpu-baseline"], timeout=300))
         print(json.dumps(line))
     ctx.close()
     plan.close()

@@ -155,6 +155,8 @@ SIGNATURES = {
                                ctypes.POINTER(_SZ)]),
     "bw_server_drain": (_I, [_P, _I]),
     "bw_server_get_stats": (_I, [_P, ctypes.POINTER(bw_server_stats)]),
+    "bw_butterfly_rate": (_I, [_I, _I, _I, ctypes.POINTER(ctypes.c_float),
+                               ctypes.POINTER(ctypes.c_double)]),
 }
 
 

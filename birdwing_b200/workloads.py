@@ -62,3 +62,72 @@ def serving_sizes(count, seed=5, lo_log=10, hi_log=24, square_frac=0.2):
         else:
             out.append((la, (max(1, int(ba * ratio[i])) + 31) // 32, False))
     return out
+
+
+# ---------------------------------------------------------------- plain products
+# The single-product workloads the benchmark times, with the exact plan
+# arguments it passes to bw_plan_create.  The parity tests build their plans
+# from the same entries, so the algorithm that is timed and the one that is
+# tested cannot drift apart.  Fields:
+#   words_a, words_b  operand lengths in u32 words (uniform random, top bit set)
+#   seeds             mt19937_64 seeds of the two operands (the reference's
+#                     1234 / 5678, tests/test_full_multiply.cpp:61-73)
+#   square            the second operand is the first (one forward transform)
+#   plan              (path, num_primes, flags) given to bw_plan_create; the
+#                     library's own choice where num_primes is 0
+#   expect            what that plan must resolve to (bw_plan_info fields)
+#   ref               (path, num_primes) of the reference's algorithm for the
+#                     same product, which the CPU restatement runs
+#   literal           (path, num_primes, flags) of the workload as the
+#                     reference states it (its coefficient width and prime
+#                     count), timed beside the library's choice
+PLAIN = {
+    "2": dict(
+        words_a=1 << 23, words_b=1 << 23, seeds=(1234, 5678), square=False,
+        plan=(BW_PATH_P64, 0, 0),
+        expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=23, log_cols=12),
+        ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
+        desc="plain 2^28-bit x 2^28-bit product"),
+    "2sq": dict(
+        words_a=1 << 23, words_b=1 << 23, seeds=(1234, 1234), square=True,
+        plan=(BW_PATH_P64, 0, 0),
+        expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=23, log_cols=12),
+        ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
+        desc="squaring of a 2^28-bit integer"),
+    "1": dict(
+        words_a=1 << 15, words_b=1 << 15, seeds=(1234, 5678), square=False,
+        plan=(BW_PATH_P32, 3, 0),
+        expect=dict(path=32, coeff_bits=16, num_primes=3, log_n=17),
+        ref=(32, 3), literal=(BW_PATH_P32, 3, 0),
+        desc="plain 2^20-bit x 2^20-bit product, 16-bit coefficients, n=2^17, "
+             "3 x 30-bit primes"),
+    "4": dict(
+        words_a=1 << 28, words_b=1 << 28, seeds=(1234, 5678), square=False,
+        plan=(BW_PATH_P64, 0, 0),
+        expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=28),
+        ref=(64, 3), literal=(BW_PATH_P64, 3, 0),
+        desc="plain huge 2^33-bit x 2^33-bit product (1 GiB operands), three-pass schedule"),
+    # a smaller product of the same kernels, for ncu captures (working set > L2)
+    "prof": dict(
+        words_a=1 << 21, words_b=1 << 21, seeds=(1234, 5678), square=False,
+        plan=(BW_PATH_P64, 0, 0),
+        expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=21),
+        ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
+        desc="plain 2^26-bit x 2^26-bit product (profiling size)"),
+}
+
+
+def plain_plan_args(name, which="plan"):
+    """(la, lb, path, num_primes, flags) of a plain workload's plan: the
+    benchmarked one (which="plan") or the reference's literal statement of
+    the workload (which="literal")."""
+    w = PLAIN[name]
+    path, k, flags = w[which]
+    return w["words_a"], w["words_b"], path, k, flags
+
+
+def algorithm_of(info):
+    """One-line description of what a plan runs, from bw_plan_info fields."""
+    prime_bits = 62 if info["path"] == 64 else 30
+    return (f"{info['coeff_bits']}-bit coefficients, n=2^{info['log_n']}, "
+            f"{info['num_primes']} x {prime_bits}-bit primes ({info['path']}-bit prime path)")

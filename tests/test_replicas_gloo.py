@@ -88,16 +88,27 @@ def test_reference_arm_line_on_rank_zero(monkeypatch):
     assert line["cpu_baseline"]["kind"] == "port"
 
 
-def test_bench_configs_split_library_and_reference_primes():
+def test_bench_configs_come_from_the_shared_table():
     """Plain configurations name the reference's algorithm (path, primes) for
-    the oracle and the CPU baseline; the library's plan takes PLAN_PRIMES
-    (0: its own choice) and reports what it chose."""
+    the oracle and the CPU baseline; the library's plan comes from the same
+    table (birdwing_b200.workloads.PLAIN) that the full-size parity tests
+    build their plans from."""
     import bench
-    assert set(bench.PLAN_PRIMES) <= set(bench.CONFIGS)
-    for name, (la, lb, path, K, square, desc) in bench.CONFIGS.items():
-        assert path in (32, 64) and K in (2, 3) and la > 0 and lb > 0
-        assert bench.PLAN_PRIMES.get(name, K) in (0, 2, 3)
-        if name in bench.PLAN_PRIMES:
-            assert "reference algorithm" in desc
+    from birdwing_b200 import workloads
+    assert set(bench.CONFIGS) == set(workloads.PLAIN)
+    for name, w in workloads.PLAIN.items():
+        la, lb, path, K, square, desc = bench.CONFIGS[name]
+        assert (la, lb, square) == (w["words_a"], w["words_b"], w["square"])
+        assert (path, K) == w["ref"] and K in (2, 3) and path in (32, 64)
+        assert w["plan"][1] in (0, 2, 3) and w["literal"][1] in (2, 3)
+        assert set(w["expect"]) <= {"path", "coeff_bits", "num_primes", "log_n", "log_cols"}
+        assert workloads.plain_plan_args(name)[:2] == (la, lb)
+        assert "reference algorithm" in bench.ref_algorithm(name)
     mb = bench.model_bytes(1 << 23, 1 << 23, 1 << 23, 3, 8, False)
     assert sum(mb.values()) == 12 * 3 * (1 << 23) * 8 + 4 * (2 << 23) * 2
+    # the fixed model of the 2^28-bit workload: K = 2, n = 2^24, w = 8
+    fixed, K, n, w = bench.fixed_model("2")
+    assert (K, n, w) == (2, 1 << 24, 8)
+    assert fixed == 12 * 2 * (1 << 24) * 8 + 4 * (2 << 23) * 2
+    info = {"num_primes": 3, "log_n": 23}
+    assert bench.plan_butterflies(info, False) == 3 * 3 * (1 << 22) * 23
