@@ -420,12 +420,13 @@ def batch_items(cfg, rank):
 
 
 def plain_launches(path, la, lb):
-    """Kernels one plain product launches: the four passes, plus the carry
-    boundary pre-pass when the output spans more than one 2048-word tile."""
+    """Kernels one plain product launches: the three transform passes, then
+    the boundary pre-pass, the words pass and the carry fix when the output
+    spans more than one 2048-word tile (the words pass alone otherwise)."""
     cpw = 2 if path == 32 else 1
     log_n = max(4, ((la + lb) * cpw - 2).bit_length())
     words = max((1 << log_n) // cpw, la + lb)
-    return 4 + (1 if words > 2048 else 0)
+    return 3 + (3 if words > 2048 else 1)
 
 
 def batch_model_bytes(items, K, small_max=None):
@@ -966,6 +967,16 @@ def fixed_model(cfg):
     return (9 if square else 12) * K * n * w + io, K, n, w
 
 
+def plain_launches_of(info, la, lb):
+    """Kernels one plain product launches: the forward column, row and inverse
+    column passes (two middle-column passes more in the three-pass
+    schedule), and Garner + carry: the boundary pre-pass, the words pass and
+    the carry fix when the output spans more than one 2048-word tile, else
+    the words pass alone."""
+    log_r2 = info["log_n"] - info["log_rows"] - info["log_cols"]
+    return 3 + (2 if log_r2 > 0 else 0) + (3 if la + lb > 2048 else 1)
+
+
 def plan_butterflies(info, square):
     """Butterflies of one product: T transforms (3, or 2 when squaring) of K
     primes, each (n/2) log2 n."""
@@ -1269,7 +1280,7 @@ def bench_plain(args):
                     "blocking_pageable_value": job_throughput(min(args.e2e_steps, 3), world,
                                                               e2e_pg_total),
                     "correct_vs_gmp": ok_e2e},
-            "gpu_launches": (5 if (la + lb) > 2048 else 4) * args.steps,
+            "gpu_launches": plain_launches_of(info, la, lb) * args.steps,
             "clocks": clocks,
         }
         if literal:

@@ -201,7 +201,7 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
     T* rb = static_cast<T*>(g.res_b);
     if (pl.small) {
         const int n = 1 << pl.log_n;
-        const size_t smem = (size_t)2 * n * sizeof(T);
+        const size_t smem = 2 * tile_elems(n) * sizeof(T);
         const int want = std::min(256, std::max(64, n >> 4));
         if (want >= 256) {
             ks_product<Ar, SPLIT16, 256><<<np, 256, smem, s>>>(P, g.d_desc, ra, g.d_err);
@@ -214,12 +214,12 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
     }
     const int R = 1 << pl.log_r, C = 1 << pl.log_c, CB = 1 << pl.log_cb;
     const int CB1 = 1 << pl.log_cb1;
-    const size_t smem1 = (size_t)R * CB1 * (sizeof(T) + (SPLIT16 ? 2 : 4));
+    const size_t smem1 = tile_elems((size_t)R * CB1) * sizeof(T) + (size_t)R * CB1 * (SPLIT16 ? 2 : 4);
     kb_fwd_col<Ar, SPLIT16, 4><<<dim3(C / CB1, 1, 2 * np), kColThreads, smem1, s>>>(
         P, g.d_desc, ra, rb);
     const int la = pl.log_c / 2;
     const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
-    const size_t smem2 = ntab * sizeof(Tw<T>) + (size_t)C * sizeof(T) * 2;
+    const size_t smem2 = ntab * sizeof(Tw<T>) + tile_elems(C) * sizeof(T) * 2;
     const dim3 g2(R, pl.K, np);
     switch (std::min(512, std::max(64, C >> 4))) {
         case 512: kb_row<Ar, 512, 4><<<g2, 512, smem2, s>>>(P, g.d_desc, ra, rb); break;
@@ -227,7 +227,7 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
         case 128: kb_row<Ar, 128, 4><<<g2, 128, smem2, s>>>(P, g.d_desc, ra, rb); break;
         default: kb_row<Ar, 64, 4><<<g2, 64, smem2, s>>>(P, g.d_desc, ra, rb); break;
     }
-    const size_t smem3 = (size_t)R * CB * sizeof(T);
+    const size_t smem3 = tile_elems((size_t)R * CB) * sizeof(T);
     kb_inv_col<Ar, 4><<<dim3(C / CB, pl.K, np), kColThreads, smem3, s>>>(P, g.d_desc, ra);
     kb_garner_carry<Ar, SPLIT16><<<dim3((unsigned)g.ntiles, np), kCarryThreads, 0, s>>>(
         P, g.d_desc, ra, 1u, g.inject_wait_fault ? 1u + (1u << 27) : 1u, g.d_err, g.spin_limit);

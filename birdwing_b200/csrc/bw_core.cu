@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -405,12 +406,19 @@ static int resolve_plan(int path, int num_primes, size_t la, size_t lb, unsigned
     return BW_OK;
 }
 
-// Streaming multiprocessors of the current device (148 on a B200).
+// Streaming multiprocessors of the current device (148 on a B200), looked up
+// once per device.
 static unsigned sm_count() {
+    static std::atomic<unsigned> cache[64];
     int dev = 0, n = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (dev >= 0 && dev < 64) {
+        const unsigned c = cache[dev].load(std::memory_order_relaxed);
+        if (c) return c;
+    }
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
         return 148;
+    if (dev >= 0 && dev < 64) cache[dev].store((unsigned)n, std::memory_order_relaxed);
     return (unsigned)n;
 }
 
@@ -489,7 +497,7 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         const size_t tsb = pl->tw_smem_r ? ((size_t)2 * w << pl->log_r) : 0;
         auto fits1 = [&](int cb) {
             const size_t elems = (size_t)1 << (pl->log_r + cb);
-            return (w + cbytes) * elems + tsb <= (wide ? 196608 : 114688);
+            return w * tile_elems(elems) + cbytes * elems + tsb <= (wide ? 196608u : 114688u);
         };
         int log_cb1 = 0;
         while (log_cb1 < log_cols_outer && fits1(log_cb1 + 1)) ++log_cb1;
@@ -862,10 +870,13 @@ template <class Ar, int RLOG>
 void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
                 const typename Ar::T* rb, int sq, size_t smem, cudaStream_t s) {
     dim3 g(1u << (pl->log_r + pl->log_r2), pl->K);
-    // one thread per sub-problem of a round, 64..512 threads (radix-8 rounds:
-    // at most 256, each thread taking several sub-problems, so that the CTA's
-    // registers leave room for more than one CTA per SM)
-    const int want = std::min(RLOG == 3 ? 256 : 512, std::max(64, 1 << (pl->log_c - RLOG)));
+    // one thread per sub-problem of a round, 64..512 threads (radix-8 rounds,
+    // and radix-16 rounds on the 32-bit path: at most 256, each thread taking
+    // several sub-problems, so that the CTA's registers leave room for more
+    // than one CTA per SM; 2^13-point rows on the 32-bit path ran one 512-thread
+    // CTA per SM at 70 registers)
+    const int cap = (RLOG == 3 || sizeof(typename Ar::T) == 4) ? 256 : 512;
+    const int want = std::min(cap, std::max(64, 1 << (pl->log_c - RLOG)));
     switch (want) {
         case 512: k_row<Ar, 512, RLOG><<<g, 512, smem, s>>>(pd, ra, rb, sq); break;
         case 256: k_row<Ar, 256, RLOG><<<g, 256, smem, s>>>(pd, ra, rb, sq); break;
@@ -979,15 +990,15 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     // the 64-bit path stages the coefficients inside the residue tile and
     // runs one prime per CTA (grid.y); the 32-bit path keeps a u16 copy
     constexpr bool PP = sizeof(T) == 8;
-    const size_t smem1 =
-        tw_bytes + (size_t)R * CB1 * (sizeof(T) + (PP ? 0 : SPLIT16 ? 2 : W64 ? 8 : 4));
+    const size_t smem1 = tw_bytes + tile_elems((size_t)R * CB1) * sizeof(T) +
+                         (size_t)R * CB1 * (PP ? 0 : SPLIT16 ? 2 : W64 ? 8 : 4);
     // K1 takes coefficient counts, or word counts for 64-bit coefficients
     const size_t in_a = W64 ? pl->la : pl->nca, in_b = W64 ? pl->lb : pl->ncb;
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
     const int tiles1 = cols_outer / CB1;
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     auto k1 = [&](int tile0, int ntiles) {
-        dim3 g1(ntiles, PP ? pl->K : 1, square ? 1 : 2);
+        dim3 g1(ntiles * (PP ? pl->K : 1), 1, square ? 1 : 2);
         if constexpr (PP) {
             if (pl->rlog_col == 3) {
                 if (ts) {
@@ -1039,7 +1050,7 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     // three passes: middle column pass with the outer twiddle
     const int CB2 = 1 << pl->log_cb2;
     const size_t smem_mid = (((size_t)1 << pl->log_r2) + CB2) * sizeof(Tw<T>) +
-                            ((size_t)CB2 << pl->log_r2) * sizeof(T);
+                            tile_elems((size_t)CB2 << pl->log_r2) * sizeof(T);
     if (pl->log_r2) {
         dim3 gm(C / CB2, R, pl->K * (square ? 1 : 2));
         k_mid_col<Ar, false><<<gm, kColThreads, smem_mid, c->stream>>>(pd, ra, rb);
@@ -1048,7 +1059,7 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
 
     const int la = pl->log_c / 2;
     const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
-    const size_t smem2 = ntab * sizeof(Tw<T>) + (size_t)C * sizeof(T) * (square ? 1 : 2);
+    const size_t smem2 = ntab * sizeof(Tw<T>) + tile_elems(C) * sizeof(T) * (square ? 1 : 2);
     const T* rbs = square ? ra : rb;
     const int sq = square ? 1 : 0;
     if (pl->rlog_row == 3) {
@@ -1062,7 +1073,7 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
         dim3 gm(C / CB2, R, pl->K);
         k_mid_col<Ar, true><<<gm, kColThreads, smem_mid, c->stream>>>(pd, ra, ra);
     }
-    const size_t smem3 = tw_bytes + (size_t)R * CB * sizeof(T);
+    const size_t smem3 = tw_bytes + tile_elems((size_t)R * CB) * sizeof(T);
     dim3 g3(cols_outer / CB, pl->K);
     bool inv_done = false;
     if constexpr (PP) {
@@ -1115,6 +1126,18 @@ int enqueue_carry(bw_ctx* c, uint32_t* out, int pieces = 1) {
     const size_t per = (c->ntiles + pieces - 1) / pieces;
     c->out_pieces = 0;
     c->out_tiles_per = per;
+    if (pieces == 1 && !c->inject_wait_fault) {
+        // one piece: the words pass (no waits between tiles) and the carry
+        // fix; the look-back form below stays for pieces that are copied out
+        // one by one and for the fault-injection hook, whose waits it tests
+        k_garner_words<Ar, SPLIT16, W64><<<(unsigned)c->ntiles, kCarryThreads, 0, c->stream>>>(
+            pd, reinterpret_cast<const T*>(c->d_res_a), out, M, NL, c->rec_x, c->rec_s, c->err);
+        if (c->ntiles > 1)
+            k_carry_fix<<<1, kFixThreads, 0, c->stream>>>(c->rec_s, (uint32_t)c->ntiles, out, M);
+        c->out_pieces = 1;
+        BW_CUDA(cudaGetLastError());
+        return BW_OK;
+    }
     for (size_t t0 = 0; t0 < c->ntiles; t0 += per) {
         const unsigned nb = (unsigned)std::min(per, c->ntiles - t0);
         k_garner_carry<Ar, SPLIT16, W64><<<nb, kCarryThreads, 0, c->stream>>>(

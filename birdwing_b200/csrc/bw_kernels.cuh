@@ -117,14 +117,38 @@ struct BatchProd {
 
 // ------------------------------------------------------------------ helpers
 
-template <typename T>
-__device__ __forceinline__ int swz(int e) {
-    if constexpr (sizeof(T) == 8) {
-        return e ^ ((e >> 4) & 15);
-    } else {
-        return e ^ ((e >> 4) & 31);
+// Shared-memory layouts of a tile: element e lives at e + MUL (e >> SH), one
+// or two pad slots after every 2^SH elements (1/16 extra either way).  A
+// round's sub-problem reads elements E0 + k 2^D (k < 2^RL, the bits of k clear
+// of E0's), whose physical indices are p(E0) + p(k 2^D): for D >= SH (and
+// D == 0) that is p(E0) + k S with one stride S = 2^D + MUL 2^(D - SH) per
+// round, so an access costs one add instead of a swizzle computation; the
+// other rounds compute their offsets.  Each kernel's tile is private, so each
+// takes the layout whose strides suit its rounds (a model of the warp's
+// accesses, bank by bank):
+//   LayRow = e + e/16: conflict-free for 8-byte residues at every stride; for
+//     4-byte residues one 2-way conflict per warp access at strides >= 32.
+//   e + 2 (e/32), 4-byte column tiles (1-8 columns): conflict-free there.
+// (An XOR swizzle, conflict-free, measured more ALU work per access in these
+// issue-bound kernels.)
+template <int SH, int MUL>
+struct Lay {
+    static __device__ __forceinline__ int p(int e) { return e + MUL * (e >> SH); }
+    static __device__ __forceinline__ bool lin(int D) { return D >= SH || D == 0; }
+    static __device__ __forceinline__ int stride(int D) {
+        return D >= SH ? (1 << D) + MUL * (1 << (D - SH)) : 1;
     }
-}
+    // offset of element k of a sub-problem at round stride D: p(k 2^D)
+    template <bool LIN>
+    static __device__ __forceinline__ int off(int k, int D, int S) {
+        return LIN ? k * S : (k << D) + MUL * ((k << D) >> SH);
+    }
+};
+using LayRow = Lay<4, 1>;
+template <typename T>
+using LayCol = typename std::conditional<sizeof(T) == 4, Lay<5, 2>, Lay<4, 1>>::type;
+// Elements of a padded tile of n logical elements (either layout).
+__host__ __device__ constexpr size_t tile_elems(size_t n) { return n + (n >> 4); }
 
 __device__ __forceinline__ uint32_t bitrev(uint32_t x, int bits) {
     return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
@@ -258,13 +282,18 @@ __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
 }
 
 // One round over all sub-problems of a batch of 2^log_cb vectors of length
-// 2^log_len.  ld(v, idx) / st(v, idx, val) move element idx of vector v.
-template <class Ar, int RL, bool INV, bool TS, class LD, class ST>
+// 2^log_len.  ld(v, idx, p) / st(v, idx, p, val) move element idx of vector v,
+// whose shared-memory tile slot is p (tile element (idx << log_cb) + v in
+// layout L).  LIN: the round's stride D = d + log_cb lets the slots advance
+// by a fixed stride (L::stride); otherwise each offset is computed (L::off).
+template <class Ar, class L, int RL, bool INV, bool TS, bool LIN, class LD, class ST>
 __device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
                                           const Tw<typename Ar::T>* __restrict__ W,
                                           const Ar& ar, bool zt, LD ld, ST st) {
     using T = typename Ar::T;
     const int d_log = log_len - s0 - RL;
+    const int D = d_log + log_cb;
+    const int S = L::stride(D);
     const int nsub = 1 << (log_cb + log_len - RL);
     for (int sp = threadIdx.x; sp < nsub; sp += blockDim.x) {
         const int v = sp & ((1 << log_cb) - 1);
@@ -272,34 +301,43 @@ __device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
         const int j = rest & ((1 << d_log) - 1);
         const int g = rest >> d_log;
         const int base = (g << (d_log + RL)) + j;
+        const int p0 = L::p((base << log_cb) + v);
         T x[1 << RL];
 #pragma unroll
-        for (int k = 0; k < (1 << RL); ++k) x[k] = ld(v, base + (k << d_log));
+        for (int k = 0; k < (1 << RL); ++k)
+            x[k] = ld(v, base + (k << d_log), p0 + L::template off<LIN>(k, D, S));
         if constexpr (!INV) {
             ct_stages<Ar, RL, TS>(x, s0, g, W, ar, zt);
         } else {
             gs_stages<Ar, RL, TS>(x, s0, g, W, ar);
         }
 #pragma unroll
-        for (int k = 0; k < (1 << RL); ++k) st(v, base + (k << d_log), x[k]);
+        for (int k = 0; k < (1 << RL); ++k)
+            st(v, base + (k << d_log), p0 + L::template off<LIN>(k, D, S), x[k]);
     }
 }
 
-// Dispatch on the round's radix: only the remainder round (the first round of
-// a transform) is narrower than 2^RLOG, so the full radix has one
-// instantiation per call site and the narrow ones stay small.
-template <class Ar, int RLOG, bool INV, bool TS, class LD, class ST>
+// Dispatch on the round's radix and addressing: only the remainder round (the
+// first round of a transform) is narrower than 2^RLOG, so the full radix has
+// one instantiation per call site and the narrow ones stay small; a round
+// whose stride the layout cannot step through linearly computes its offsets.
+template <class Ar, class L, int RLOG, bool INV, bool TS, class LD, class ST>
 __device__ __forceinline__ void run_round_rl(int rl, int log_len, int log_cb, int s0,
                                              const Tw<typename Ar::T>* __restrict__ W,
                                              const Ar& ar, bool zt, LD ld, ST st) {
+    const int D = log_len - s0 - rl + log_cb;
     if (rl == RLOG) {
-        run_round<Ar, RLOG, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        if (L::lin(D)) {
+            run_round<Ar, L, RLOG, INV, TS, true>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        } else {
+            run_round<Ar, L, RLOG, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        }
     } else if (rl == 3) {
-        run_round<Ar, 3, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        run_round<Ar, L, 3, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
     } else if (rl == 2) {
-        run_round<Ar, 2, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        run_round<Ar, L, 2, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
     } else {
-        run_round<Ar, 1, INV, TS>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        run_round<Ar, L, 1, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
     }
 }
 
@@ -346,52 +384,75 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
 
     Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
     T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
-    CT* coef = reinterpret_cast<CT*>(buf + (R << log_cb));
+    CT* coef = reinterpret_cast<CT*>(buf + tile_elems((size_t)R << log_cb));
 
-    for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
-        const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
-        if constexpr (PP) {
-            // into the residue tile at the first round's (swizzled) slot
-            uint32_t* dst = reinterpret_cast<uint32_t*>(buf + swz<T>(e));
-            const size_t wi = W64 ? 2 * ci : ci;
-            if (wi < ncoef) {
-                cp_async_elem(dst, limbs + wi);
-            } else {
-                dst[0] = 0;
-            }
-            if (W64 && wi + 1 < ncoef) {
-                cp_async_elem(dst + 1, limbs + wi + 1);
-            } else {
-                dst[1] = 0;
-            }
-        } else if constexpr (SPLIT16) {
-            const uint32_t val =
-                ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu : 0u;
-            coef[e] = (CT)val;
-        } else if constexpr (W64) {
-            // two 4-byte copies: the operand may start at an odd word
-            uint32_t* dst = reinterpret_cast<uint32_t*>(coef + e);
-            const size_t wi = 2 * ci;
-            if (wi < ncoef) {
-                cp_async_elem(dst, limbs + wi);
-            } else {
-                dst[0] = 0;
-            }
-            if (wi + 1 < ncoef) {
-                cp_async_elem(dst + 1, limbs + wi + 1);
-            } else {
-                dst[1] = 0;
+    if constexpr (SPLIT16) {
+        if (CB >= 2) {
+            // whole limbs (two 16-bit coefficients each) by cp.async into the
+            // u16 tile: limb e of the tile holds its coefficients 2e and
+            // 2e + 1, exactly the little-endian u16 layout the first round
+            // reads (CB is even and C is even, so every row segment is whole
+            // limbs)
+            const int hcb = CB >> 1;
+            uint32_t* coef32 = reinterpret_cast<uint32_t*>(coef);
+            const size_t nlimbs = (ncoef + 1) >> 1;
+            for (int e = threadIdx.x; e < rows_loaded * hcb; e += blockDim.x) {
+                const size_t li = ((size_t)(e / hcb) * C + c0) / 2 + (e % hcb);
+                if (li < nlimbs) {
+                    cp_async_elem(coef32 + e, limbs + li);
+                } else {
+                    coef32[e] = 0;
+                }
             }
         } else {
-            // 32-bit limbs land in shared memory without passing registers
-            if (ci < ncoef) {
-                cp_async_elem(coef + e, limbs + ci);
+            for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
+                const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
+                coef[e] = (CT)(ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu
+                                          : 0u);
+            }
+        }
+    } else {
+        for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
+            const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
+            if constexpr (PP) {
+                // into the residue tile at the first round's (swizzled) slot
+                uint32_t* dst = reinterpret_cast<uint32_t*>(buf + LayCol<T>::p(e));
+                const size_t wi = W64 ? 2 * ci : ci;
+                if (wi < ncoef) {
+                    cp_async_elem(dst, limbs + wi);
+                } else {
+                    dst[0] = 0;
+                }
+                if (W64 && wi + 1 < ncoef) {
+                    cp_async_elem(dst + 1, limbs + wi + 1);
+                } else {
+                    dst[1] = 0;
+                }
+            } else if constexpr (W64) {
+                // two 4-byte copies: the operand may start at an odd word
+                uint32_t* dst = reinterpret_cast<uint32_t*>(coef + e);
+                const size_t wi = 2 * ci;
+                if (wi < ncoef) {
+                    cp_async_elem(dst, limbs + wi);
+                } else {
+                    dst[0] = 0;
+                }
+                if (wi + 1 < ncoef) {
+                    cp_async_elem(dst + 1, limbs + wi + 1);
+                } else {
+                    dst[1] = 0;
+                }
             } else {
-                coef[e] = 0;
+                // 32-bit limbs land in shared memory without passing registers
+                if (ci < ncoef) {
+                    cp_async_elem(coef + e, limbs + ci);
+                } else {
+                    coef[e] = 0;
+                }
             }
         }
     }
-    if constexpr (!SPLIT16) cp_async_wait();
+    cp_async_wait();
 
     const int nr = sched_rounds<RLOG>(log_r);
     for (int kp = PP ? kp0 : 0; kp < (PP ? kp0 + 1 : P.K); ++kp) {
@@ -409,10 +470,10 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             const bool first = (r == 0), last = (r == nr - 1);
             // first round reads the coefficient tile (zero pad virtual), last
             // round writes to global memory
-            auto ld = [&](int v, int idx) -> T {
+            auto ld = [&](int v, int idx, int p) -> T {
                 if (first) {
                     if (zt && idx >= R / 2) return T(0);
-                    T x = PP ? buf[swz<T>((idx << log_cb) + v)] : (T)coef[(idx << log_cb) + v];
+                    T x = PP ? buf[p] : (T)coef[(idx << log_cb) + v];
                     if constexpr (W64) {
                         // 2^64 < 6.0001 p: two conditional 3p steps reach [0, 3p)
                         x = min(x, x - ar.p3);
@@ -420,16 +481,16 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                     }
                     return x;
                 }
-                return buf[swz<T>((idx << log_cb) + v)];
+                return buf[p];
             };
-            auto st = [&](int v, int idx, T val) {
+            auto st = [&](int v, int idx, int p, T val) {
                 if (last) {
                     gout[(size_t)idx * C + c0 + v] = val;
                 } else {
-                    buf[swz<T>((idx << log_cb) + v)] = val;
+                    buf[p] = val;
                 }
             };
-            run_round_rl<Ar, RLOG, false, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
+            run_round_rl<Ar, LayCol<T>, RLOG, false, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
                                               sched_s0<RLOG>(log_r, r), W, ar, first && zt, ld,
                                               st);
             __syncthreads();
@@ -437,7 +498,11 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
     }
 }
 
-// PP: blockIdx.y = prime (64-bit path).  Three CTAs per SM (at most 85
+// PP (64-bit path): blockIdx.x = tile * K + prime, so the K CTAs of one tile
+// are launched next to each other and run together: the first brings the
+// tile's operand words into L2 and the others read them from there (with the
+// prime as grid.y, the residue writes of the tiles in between evicted them and
+// every prime re-read its operands from DRAM).  Three CTAs per SM (at most 85
 // registers; the 64-bit kernels then spill 32-80 bytes to the stack): the
 // shared-memory tile allows three, and the 2^28-bit product measured K1 4%
 // faster than at two (the inverse pass measured slower with the same bound).
@@ -450,8 +515,9 @@ k_fwd_col(const PlanDev<Ar> P, const uint32_t* __restrict__ limbs_a, size_t ncoe
     const int op = blockIdx.z;
     fwd_col_body<Ar, SPLIT16, RLOG, TS, W64, PP>(P, op ? limbs_b : limbs_a,
                                                  op ? ncoef_b : ncoef_a, op ? res_b : res_a,
-                                                 (zt_mask >> op) & 1u, tile0 + (int)blockIdx.x,
-                                                 smem_raw, PP ? (int)blockIdx.y : 0);
+                                                 (zt_mask >> op) & 1u,
+                                                 tile0 + (int)(PP ? blockIdx.x / P.K : blockIdx.x),
+                                                 smem_raw, PP ? (int)(blockIdx.x % P.K) : 0);
 }
 
 // batched: blockIdx.z = 2 * product + operand
@@ -510,7 +576,7 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     Tw<T>* Fi = G + ng;
     Tw<T>* Gi = Fi + nf;
     T* bufA = reinterpret_cast<T*>(Gi + ng);
-    T* bufB = bufA + C;
+    T* bufB = bufA + tile_elems(C);
 
     const uint64_t k1 = bitrev((uint32_t)prow & ((1u << log_rr) - 1), log_rr);
     const uint64_t nmask = n_row - 1;
@@ -534,13 +600,13 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     // the in-place twiddle then costs one more shared-memory pass)
     for (int i = threadIdx.x; i < C; i += NT) {
         const Tw<T> f = F[i & (nf - 1)], g = G[i >> la];
-        bufA[swz<T>(i)] = ar.mulc(ar.mulc(ga[i], f.w, f.wq), g.w, g.wq);
-        if (!square) bufB[swz<T>(i)] = ar.mulc(ar.mulc(gb[i], f.w, f.wq), g.w, g.wq);
+        bufA[LayRow::p(i)] = ar.mulc(ar.mulc(ga[i], f.w, f.wq), g.w, g.wq);
+        if (!square) bufB[LayRow::p(i)] = ar.mulc(ar.mulc(gb[i], f.w, f.wq), g.w, g.wq);
     }
     __syncthreads();
 
     const int nr = sched_rounds<RLOG>(log_c);
-    auto ldA = [&](int, int idx) -> T { return bufA[swz<T>(idx)]; };
+    auto ldA = [&](int, int, int p) -> T { return bufA[p]; };
     auto st_glob = [&](int idx, T v) {
         const Tw<T> f = Fi[idx & (nf - 1)], g = Gi[idx >> la];
         ga[idx] = ar.mulc(ar.mulc(v, f.w, f.wq), g.w, g.wq);
@@ -551,10 +617,10 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     for (int op = 0; op < (square ? 1 : 2); ++op) {
         T* buf = op ? bufB : bufA;
         const int rounds = (op == 0 && !square) ? nr : nr - 1;
-        auto ld = [&](int, int idx) -> T { return buf[swz<T>(idx)]; };
-        auto st = [&](int, int idx, T v) { buf[swz<T>(idx)] = v; };
+        auto ld = [&](int, int, int p) -> T { return buf[p]; };
+        auto st = [&](int, int, int p, T v) { buf[p] = v; };
         for (int r = 0; r < rounds; ++r) {
-            run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
+            run_round_rl<Ar, LayRow, RLOG, false, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
                                                  sched_s0<RLOG>(log_c, r), pr.WCf, ar, false,
                                                  ld, st);
             __syncthreads();
@@ -562,7 +628,9 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     }
 
     // fused round: last forward round of B (or A), pointwise product, first
-    // inverse round -- one sub-problem stays in registers throughout.
+    // inverse round -- one sub-problem stays in registers throughout.  The
+    // last round of the schedule has stride 1 (d_log = 0), so the slots of a
+    // sub-problem are swz(base) + k.
     {
         const int r = nr - 1;
         const int rl = sched_rl<RLOG>(log_c, r), s0 = sched_s0<RLOG>(log_c, r);
@@ -574,21 +642,20 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
             const int j = sp & ((1 << d_log) - 1);
             const int g = sp >> d_log;
             const int base = (g << (d_log + rl)) + j;
+            const int p0 = LayRow::p(base);
             T x[1 << RLOG];
 #define BW_FUSED_BODY(RL)                                                              \
     {                                                                                  \
-        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] =                   \
-            src[swz<T>(base + (k << d_log))];                                          \
+        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] = src[p0 + k];     \
         ct_stages<Ar, RL, false>(x, s0, g, pr.WCf, ar, false);                         \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
             const T xa = ar.fwd_to_2p(x[k]);                                           \
-            const T ya = square ? xa : ar.fwd_to_2p(bufA[swz<T>(base + (k << d_log))]); \
+            const T ya = square ? xa : ar.fwd_to_2p(bufA[p0 + k]);                     \
             x[k] = ar.mont(xa, ya);                                                    \
         }                                                                              \
         gs_stages<Ar, RL, false>(x, s0, g, pr.WCi, ar);                                \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
-            const int idx = base + (k << d_log);                                       \
-            if (final_round) st_glob(idx, x[k]); else bufA[swz<T>(idx)] = x[k];        \
+            if (final_round) st_glob(base + k, x[k]); else bufA[p0 + k] = x[k];        \
         }                                                                              \
     }
             if (rl == RLOG) {
@@ -608,14 +675,14 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     // remaining inverse rounds, the last one writes to global with the twiddle
     for (int r = nr - 2; r >= 0; --r) {
         const bool last = (r == 0);
-        auto st = [&](int, int idx, T v) {
+        auto st = [&](int, int idx, int p, T v) {
             if (last) {
                 st_glob(idx, v);
             } else {
-                bufA[swz<T>(idx)] = v;
+                bufA[p] = v;
             }
         };
-        run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
+        run_round_rl<Ar, LayRow, RLOG, true, false>(sched_rl<RLOG>(log_c, r), log_c, 0,
                                             sched_s0<RLOG>(log_c, r), pr.WCi, ar, false, ldA, st);
         __syncthreads();
     }
@@ -670,7 +737,7 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
 
     // the tile's loads first: they land while the twiddle tables are built
     for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x)
-        cp_async_elem(buf + swz<T>(e), g + ((size_t)(e >> log_cb) << log_c) + c0 + (e & (CB - 1)));
+        cp_async_elem(buf + LayCol<T>::p(e), g + ((size_t)(e >> log_cb) << log_c) + c0 + (e & (CB - 1)));
     const uint64_t k1 = bitrev((uint32_t)s, P.log_r);
     const uint64_t nmask = n - 1;
     for (int i = threadIdx.x; i < R2 + CB; i += blockDim.x) {
@@ -692,20 +759,20 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
         for (int e = threadIdx.x; e < (R2 << log_cb); e += blockDim.x) {
             const int i2 = e >> log_cb, v = e & (CB - 1);
             const Tw<T> a = Tcol[v], b = Trow[i2];
-            buf[swz<T>(e)] = ar.mulc(ar.mulc(buf[swz<T>(e)], a.w, a.wq), b.w, b.wq);
+            buf[LayCol<T>::p(e)] = ar.mulc(ar.mulc(buf[LayCol<T>::p(e)], a.w, a.wq), b.w, b.wq);
         }
         __syncthreads();
         for (int r = 0; r < nr; ++r) {
             const bool last = (r == nr - 1);
-            auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
-            auto st = [&](int v, int idx, T val) {
+            auto ld = [&](int, int, int p) -> T { return buf[p]; };
+            auto st = [&](int v, int idx, int p, T val) {
                 if (last) {
                     g[((size_t)idx << log_c) + c0 + v] = val;
                 } else {
-                    buf[swz<T>((idx << log_cb) + v)] = val;
+                    buf[p] = val;
                 }
             };
-            run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
+            run_round_rl<Ar, LayCol<T>, RLOG, false, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
                                                  sched_s0<RLOG>(log_r2, r), pr.WMf, ar, false,
                                                  ld, st);
             __syncthreads();
@@ -713,17 +780,17 @@ k_mid_col(const PlanDev<Ar> P, typename Ar::T* res_a, typename Ar::T* res_b) {
     } else {
         for (int r = nr - 1; r >= 0; --r) {
             const bool last = (r == 0);
-            auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
-            auto st = [&](int v, int idx, T val) {
+            auto ld = [&](int, int, int p) -> T { return buf[p]; };
+            auto st = [&](int v, int idx, int p, T val) {
                 if (last) {
                     const Tw<T> a = Tcol[v], b = Trow[idx];
                     g[((size_t)idx << log_c) + c0 + v] =
                         ar.mulc(ar.mulc(val, a.w, a.wq), b.w, b.wq);
                 } else {
-                    buf[swz<T>((idx << log_cb) + v)] = val;
+                    buf[p] = val;
                 }
             };
-            run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
+            run_round_rl<Ar, LayCol<T>, RLOG, true, false>(sched_rl<RLOG>(log_r2, r), log_r2, log_cb,
                                                 sched_s0<RLOG>(log_r2, r), pr.WMi, ar, false, ld,
                                                 st);
             __syncthreads();
@@ -761,22 +828,22 @@ __device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::
     // the whole tile in flight at once (cp.async), then every round from
     // shared memory; the last round reduces and writes global memory
     for (int e = threadIdx.x; e < (R << log_cb); e += blockDim.x)
-        cp_async_elem(buf + swz<T>(e), g + (size_t)(e >> log_cb) * C + c0 + (e & ((1 << log_cb) - 1)));
+        cp_async_elem(buf + LayCol<T>::p(e), g + (size_t)(e >> log_cb) * C + c0 + (e & ((1 << log_cb) - 1)));
     cp_async_wait();
     __syncthreads();
 
     const int nr = sched_rounds<RLOG>(log_r);
     for (int r = nr - 1; r >= 0; --r) {
         const bool last = (r == 0);
-        auto ld = [&](int v, int idx) -> T { return buf[swz<T>((idx << log_cb) + v)]; };
-        auto st = [&](int v, int idx, T val) {
+        auto ld = [&](int, int, int p) -> T { return buf[p]; };
+        auto st = [&](int v, int idx, int p, T val) {
             if (last) {
                 g[(size_t)idx * C + c0 + v] = ar.inv_out(val);
             } else {
-                buf[swz<T>((idx << log_cb) + v)] = val;
+                buf[p] = val;
             }
         };
-        run_round_rl<Ar, RLOG, true, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
+        run_round_rl<Ar, LayCol<T>, RLOG, true, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
                                          sched_s0<RLOG>(log_r, r), W, ar, false, ld, st);
         __syncthreads();
     }
@@ -826,11 +893,14 @@ kb_inv_col(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
 // sums D[e] < 2^96 (one coefficient per word, or two 16-bit ones).  Words at
 // or beyond NL read nothing and are zero.  Sets *bad when the redundant
 // third prime disagrees or a value reaches 2^96.
+// base: this thread's first residue of prime 0 (global memory, or a tile
+// staged in shared memory); prime k's residues start pstride elements later.
+// valid: the words exist (false: they read as zero).
 template <class Ar, bool SPLIT16, int E, bool NC = true>
-__device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
-                                              const typename Ar::T* __restrict__ res, size_t n,
-                                              size_t j0, size_t NL, unsigned __int128 (&D)[E],
-                                              uint32_t* bad_out) {
+__device__ __forceinline__ void garner_digits_at(const PlanDev<Ar>& P,
+                                                 const typename Ar::T* __restrict__ base,
+                                                 size_t pstride, bool valid,
+                                                 unsigned __int128 (&D)[E], uint32_t* bad_out) {
     using T = typename Ar::T;
     constexpr int CPW = SPLIT16 ? 2 : 1;
     uint32_t bad = 0;
@@ -842,13 +912,12 @@ __device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
         for (int kp = 0; kp < kMaxPrimes; ++kp)
 #pragma unroll
             for (int q = 0; q < E * CPW; ++q) r[kp][q] = 0;
-        if (j0 < NL) {
+        if (valid) {
             // 128-bit vector loads of E*CPW consecutive residues per prime
 #pragma unroll
             for (int kp = 0; kp < kMaxPrimes; ++kp) {
                 if (kp >= P.K) break;
-                const uint4* src =
-                    reinterpret_cast<const uint4*>(res + (size_t)kp * n + j0 * CPW);
+                const uint4* src = reinterpret_cast<const uint4*>(base + (size_t)kp * pstride);
 #pragma unroll
                 for (int q = 0; q < (E * CPW * (int)sizeof(T)) / 16; ++q) {
                     // NC: read-only path (residues from an earlier kernel);
@@ -900,6 +969,15 @@ __device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
     *bad_out |= bad;
 }
 
+template <class Ar, bool SPLIT16, int E, bool NC = true>
+__device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
+                                              const typename Ar::T* __restrict__ res, size_t n,
+                                              size_t j0, size_t NL, unsigned __int128 (&D)[E],
+                                              uint32_t* bad_out) {
+    garner_digits_at<Ar, SPLIT16, E, NC>(P, res + j0 * (SPLIT16 ? 2 : 1), n, j0 < NL, D,
+                                         bad_out);
+}
+
 // 64-bit coefficients (three primes): the E output words from word j0 (j0
 // even, E/2 coefficients from coefficient j0/2) and the carry-out X.  Each
 // coefficient is the full mixed-radix value c = r0 + p0 k1 + p0 p1 k2
@@ -908,11 +986,11 @@ __device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
 // the low 32 E bits of V = sum_q c_q 2^(64 q), X = V >> 32 E (< 2^96).
 // Coefficients at or beyond NL / 2 read nothing and are zero.
 template <class Ar, int E, bool NC = true>
-__device__ __forceinline__ void garner_words_w64(const PlanDev<Ar>& P,
-                                                 const typename Ar::T* __restrict__ res,
-                                                 size_t n, size_t j0, size_t NL,
-                                                 uint32_t (&l)[E], uint32_t (&X)[3],
-                                                 uint32_t* bad_out) {
+__device__ __forceinline__ void garner_words_w64_at(const PlanDev<Ar>& P,
+                                                    const typename Ar::T* __restrict__ base,
+                                                    size_t pstride, bool valid,
+                                                    uint32_t (&l)[E], uint32_t (&X)[3],
+                                                    uint32_t* bad_out) {
     using T = typename Ar::T;
     static_assert(sizeof(T) == 8 && E % 4 == 0, "64-bit residues, whole 16-byte loads");
     constexpr int Q = E / 2;
@@ -921,10 +999,10 @@ __device__ __forceinline__ void garner_words_w64(const PlanDev<Ar>& P,
     for (int kp = 0; kp < 3; ++kp)
 #pragma unroll
         for (int q = 0; q < Q; ++q) r[kp][q] = 0;
-    if (j0 < NL) {
+    if (valid) {
 #pragma unroll
         for (int kp = 0; kp < 3; ++kp) {
-            const uint4* src = reinterpret_cast<const uint4*>(res + (size_t)kp * n + j0 / 2);
+            const uint4* src = reinterpret_cast<const uint4*>(base + (size_t)kp * pstride);
 #pragma unroll
             for (int h = 0; h < Q / 2; ++h) {
                 const uint4 v = NC ? __ldg(src + h) : src[h];
@@ -969,6 +1047,15 @@ __device__ __forceinline__ void garner_words_w64(const PlanDev<Ar>& P,
     *bad_out |= bad;
 }
 
+template <class Ar, int E, bool NC = true>
+__device__ __forceinline__ void garner_words_w64(const PlanDev<Ar>& P,
+                                                 const typename Ar::T* __restrict__ res,
+                                                 size_t n, size_t j0, size_t NL,
+                                                 uint32_t (&l)[E], uint32_t (&X)[3],
+                                                 uint32_t* bad_out) {
+    garner_words_w64_at<Ar, E, NC>(P, res + j0 / 2, n, j0 < NL, l, X, bad_out);
+}
+
 // CTA-wide resolution of a 1-bit carry chain.  Each thread has a status
 // st: 0 kill, 1 propagate, 2 generate.  chain_prepare publishes per-warp
 // aggregates (carry out for carry-in 0 / 1) in s_w and must be followed by a
@@ -1007,50 +1094,26 @@ __device__ __forceinline__ uint32_t chain_mine(const ChainMasks& m, const uint32
     return (carries >> lane) & 1u;
 }
 
-template <class Ar, bool SPLIT16, bool W64 = false>
-__device__ __forceinline__ void garner_carry_body(
-    const PlanDev<Ar>& P, const typename Ar::T* __restrict__ res, uint32_t* __restrict__ out,
-    size_t M, size_t NL, CarryState* cst, uint4* __restrict__ rec_x,
+// Shared memory of one tile's carry resolution.
+struct CarryShared {
+    uint32_t w[kCarryThreads / 32];
+    uint32_t lastx[kCarryThreads / 32][3];
+    uint32_t cin[3];
+    uint32_t eps;
+};
+
+// Tile t's carry, given every thread's 8 words l (digit sums added with
+// carry-in zero) and carry-out X: publish the tile's carry words, take the
+// predecessor's, resolve the 1-bit carry chain inside the tile, publish the
+// tile status and look back across tiles, then write the final words.  Every
+// thread of the CTA calls it; it returns after its last barrier.
+__device__ __forceinline__ void carry_finish_tile(
+    uint32_t t, size_t j0, const uint32_t (&l)[kCarryWordsPerThread], const uint32_t (&X)[3],
+    uint32_t* __restrict__ out, size_t M, uint4* __restrict__ rec_x,
     uint32_t* __restrict__ rec_s, uint32_t epoch, uint32_t wait_epoch,
-    uint32_t* __restrict__ err, int spin_limit) {
-    using T = typename Ar::T;
+    uint32_t* __restrict__ err, int spin_limit, CarryShared& sh) {
     constexpr int E = kCarryWordsPerThread;
-    constexpr int TL = kCarryTileWords;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_w[kCarryThreads / 32];
-    __shared__ uint32_t s_lastx[kCarryThreads / 32][3];
-    __shared__ uint32_t s_cin[3];
-    __shared__ uint32_t s_eps;
-
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(&cst->counter, 1u);
-    __syncthreads();
-    const uint32_t t = s_tile;
-    const size_t j0 = (size_t)t * TL + (size_t)tid * E;
-    const size_t n = (size_t)1 << P.log_n;
-
-    // ---- Garner and the local carry: words l[0..E) and carry-out X < 2^96
-    uint32_t l[E];
-    uint32_t X[3];
-    uint32_t bad = 0;
-    if constexpr (W64) {
-        garner_words_w64<Ar, E>(P, res, n, j0, NL, l, X, &bad);
-    } else {
-        // digit sums D[e] < 2^96
-        unsigned __int128 D[E];
-        garner_digits<Ar, SPLIT16, E>(P, res, n, j0, NL, D, &bad);
-        unsigned __int128 acc = 0;
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            acc += D[e];
-            l[e] = (uint32_t)acc;
-            acc >>= 32;
-        }
-        X[0] = (uint32_t)acc;
-        X[1] = (uint32_t)(acc >> 32);
-        X[2] = (uint32_t)(acc >> 64);
-    }
-    if (bad) atomicOr(err, 2u);
 
     // ---- the tile's carry words: the last thread's X, published at once
     // (it depends on nothing outside the tile)
@@ -1068,12 +1131,12 @@ __device__ __forceinline__ void garner_carry_body(
 #pragma unroll
     for (int q = 0; q < 3; ++q) PX[q] = __shfl_up_sync(0xffffffffu, X[q], 1);
     if (lane == 31) {
-        s_lastx[warp][0] = X[0];
-        s_lastx[warp][1] = X[1];
-        s_lastx[warp][2] = X[2];
+        sh.lastx[warp][0] = X[0];
+        sh.lastx[warp][1] = X[1];
+        sh.lastx[warp][2] = X[2];
     }
     if (tid == 0) {
-        s_cin[0] = s_cin[1] = s_cin[2] = 0;
+        sh.cin[0] = sh.cin[1] = sh.cin[2] = 0;
         if (t > 0) {
             const uint32_t* rx = reinterpret_cast<const uint32_t*>(rec_x + (t - 1));
             int it = 0;
@@ -1083,12 +1146,12 @@ __device__ __forceinline__ void garner_carry_body(
                     ok = false;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
             if (ok) {
-                s_cin[0] = ld_relaxed(rx + 0);
-                s_cin[1] = ld_relaxed(rx + 1);
-                s_cin[2] = ld_relaxed(rx + 2);
+                sh.cin[0] = ld_relaxed(rx + 0);
+                sh.cin[1] = ld_relaxed(rx + 1);
+                sh.cin[2] = ld_relaxed(rx + 2);
             } else {
                 atomicOr(err, 1u);
             }
@@ -1097,7 +1160,7 @@ __device__ __forceinline__ void garner_carry_body(
     __syncthreads();
     if (lane == 0) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) PX[q] = warp > 0 ? s_lastx[warp - 1][q] : s_cin[q];
+        for (int q = 0; q < 3; ++q) PX[q] = warp > 0 ? sh.lastx[warp - 1][q] : sh.cin[q];
     }
 
     // ---- S = l + PX and this thread's status
@@ -1108,20 +1171,20 @@ __device__ __forceinline__ void garner_carry_body(
         uint32_t all = 0xffffffffu;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const uint64_t s = (uint64_t)l[e] + (e < 3 ? PX[e] : 0u) + c;
-            S[e] = (uint32_t)s;
-            c = s >> 32;
+            const uint64_t sum = (uint64_t)l[e] + (e < 3 ? PX[e] : 0u) + c;
+            S[e] = (uint32_t)sum;
+            c = sum >> 32;
             all &= S[e];
         }
         st = c ? 2 : (all == 0xffffffffu ? 1 : 0);
     }
 
-    const ChainMasks cm = chain_prepare(st, s_w);
+    const ChainMasks cm = chain_prepare(st, sh.w);
     __syncthreads();
 
     // ---- tile status, publish, look back (thread 0)
     if (tid == 0) {
-        const uint32_t c0 = chain_out(s_w, 0u), c1 = chain_out(s_w, 1u);
+        const uint32_t c0 = chain_out(sh.w, 0u), c1 = chain_out(sh.w, 1u);
         const uint32_t kind = c0 ? 2u : (c1 ? 1u : 0u);
         const uint32_t tag = epoch << 4;
         uint32_t eps_in = 0;
@@ -1137,7 +1200,7 @@ __device__ __forceinline__ void garner_carry_body(
                         eps_in = 0;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                     continue;
                 }
                 if (v & 8u) {
@@ -1154,20 +1217,20 @@ __device__ __forceinline__ void garner_carry_body(
         }
         const uint32_t eps_out = kind == 2u ? 1u : (kind == 1u ? eps_in : 0u);
         st_release(rec_s + t, tag | 8u | (eps_out << 2) | kind);
-        s_eps = eps_in;
+        sh.eps = eps_in;
     }
     __syncthreads();
 
     // ---- final words
-    const uint32_t mc = chain_mine(cm, s_w, s_eps);
+    const uint32_t mc = chain_mine(cm, sh.w, sh.eps);
     uint32_t w[E];
     {
         uint64_t c = mc;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const uint64_t s = (uint64_t)S[e] + c;
-            w[e] = (uint32_t)s;
-            c = s >> 32;
+            const uint64_t sum = (uint64_t)S[e] + c;
+            w[e] = (uint32_t)sum;
+            c = sum >> 32;
         }
     }
     if (j0 + E <= M && ((reinterpret_cast<uintptr_t>(out + j0) & 15u) == 0)) {
@@ -1178,6 +1241,215 @@ __device__ __forceinline__ void garner_carry_body(
 #pragma unroll
         for (int e = 0; e < E; ++e)
             if (j0 + e < M) out[j0 + e] = w[e];
+    }
+}
+
+// Words l and carry-out X of E = 8 output words from digit sums (16- and
+// 32-bit coefficients) or full coefficients (64-bit), read from `base` (this
+// thread's first residue of prime 0, primes pstride apart; global memory or a
+// shared-memory tile).
+template <class Ar, bool SPLIT16, bool W64, bool NC>
+__device__ __forceinline__ void garner_local(const PlanDev<Ar>& P,
+                                             const typename Ar::T* __restrict__ base,
+                                             size_t pstride, bool valid,
+                                             uint32_t (&l)[kCarryWordsPerThread],
+                                             uint32_t (&X)[3], uint32_t* bad) {
+    constexpr int E = kCarryWordsPerThread;
+    if constexpr (W64) {
+        garner_words_w64_at<Ar, E, NC>(P, base, pstride, valid, l, X, bad);
+    } else {
+        unsigned __int128 D[E];
+        garner_digits_at<Ar, SPLIT16, E, NC>(P, base, pstride, valid, D, bad);
+        unsigned __int128 acc = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            acc += D[e];
+            l[e] = (uint32_t)acc;
+            acc >>= 32;
+        }
+        X[0] = (uint32_t)acc;
+        X[1] = (uint32_t)(acc >> 32);
+        X[2] = (uint32_t)(acc >> 64);
+    }
+}
+
+// Residue elements of one word of output: two 16-bit coefficients, one 32-bit
+// coefficient, or half a 64-bit coefficient.
+template <bool SPLIT16, bool W64>
+__host__ __device__ constexpr size_t elems_per_word2() {
+    return SPLIT16 ? 4 : W64 ? 1 : 2;  // in halves: x2 of the element count
+}
+
+template <class Ar, bool SPLIT16, bool W64 = false>
+__device__ __forceinline__ void garner_carry_body(
+    const PlanDev<Ar>& P, const typename Ar::T* __restrict__ res, uint32_t* __restrict__ out,
+    size_t M, size_t NL, CarryState* cst, uint4* __restrict__ rec_x,
+    uint32_t* __restrict__ rec_s, uint32_t epoch, uint32_t wait_epoch,
+    uint32_t* __restrict__ err, int spin_limit) {
+    constexpr int E = kCarryWordsPerThread;
+    constexpr int TL = kCarryTileWords;
+    __shared__ uint32_t s_tile;
+    __shared__ CarryShared sh;
+
+    const int tid = threadIdx.x;
+    if (tid == 0) s_tile = atomicAdd(&cst->counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const size_t j0 = (size_t)t * TL + (size_t)tid * E;
+    const size_t n = (size_t)1 << P.log_n;
+
+    uint32_t l[E];
+    uint32_t X[3];
+    uint32_t bad = 0;
+    garner_local<Ar, SPLIT16, W64, true>(P, res + j0 * elems_per_word2<SPLIT16, W64>() / 2, n,
+                                         j0 < NL, l, X, &bad);
+    if (bad) atomicOr(err, 2u);
+    carry_finish_tile(t, j0, l, X, out, M, rec_x, rec_s, epoch, wait_epoch, err, spin_limit, sh);
+}
+
+// K4 without waits (single products).  The look-back form above keeps every
+// CTA of a tile waiting on its predecessor's records: two or three dependent
+// L2 round trips per tile with the whole CTA at a barrier.  Here the 1-bit
+// tile carry is left out of the first pass instead: k_carry_bounds has
+// already published every tile boundary's carry words X, so tile t writes its
+// words as if the carry bit eps into it were 0 and records its kind -- the
+// carry bit it passes on for eps = 0 and for eps = 1 (kill: 0/0, propagate:
+// 0/1, generate: 1/1).  k_carry_fix then scans the kinds (eps into tile 0 is
+// 0) and adds 1 at the first word of each tile whose eps is 1, rippling
+// inside the tile (a tile that propagates passes the carry on through the
+// next tile's own eps).  For operands of random words no tile but an
+// all-ones span generates or propagates, so the fix pass writes nothing.
+template <class Ar, bool SPLIT16, bool W64 = false>
+__global__ void __launch_bounds__(kCarryThreads, 4)
+k_garner_words(const PlanDev<Ar> P, const typename Ar::T* __restrict__ res,
+               uint32_t* __restrict__ out, size_t M, size_t NL,
+               const uint4* __restrict__ rec_x, uint32_t* __restrict__ kinds,
+               uint32_t* __restrict__ err) {
+    constexpr int E = kCarryWordsPerThread;
+    constexpr int TL = kCarryTileWords;
+    __shared__ CarryShared sh;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t t = blockIdx.x;
+    const size_t j0 = (size_t)t * TL + (size_t)tid * E;
+    const size_t n = (size_t)1 << P.log_n;
+    if (tid == 0) {
+        // the previous tile's boundary carry words, from the pre-pass
+        uint4 px = make_uint4(0, 0, 0, 0);
+        if (t > 0) px = __ldcg(rec_x + (t - 1));
+        sh.cin[0] = px.x;
+        sh.cin[1] = px.y;
+        sh.cin[2] = px.z;
+    }
+    uint32_t l[E];
+    uint32_t X[3];
+    uint32_t bad = 0;
+    garner_local<Ar, SPLIT16, W64, true>(P, res + j0 * elems_per_word2<SPLIT16, W64>() / 2, n,
+                                         j0 < NL, l, X, &bad);
+    if (bad) atomicOr(err, 2u);
+    uint32_t PX[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) PX[q] = __shfl_up_sync(0xffffffffu, X[q], 1);
+    if (lane == 31) {
+        sh.lastx[warp][0] = X[0];
+        sh.lastx[warp][1] = X[1];
+        sh.lastx[warp][2] = X[2];
+    }
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) PX[q] = warp > 0 ? sh.lastx[warp - 1][q] : sh.cin[q];
+    }
+    uint32_t S[E];
+    int st;
+    {
+        uint64_t c = 0;
+        uint32_t all = 0xffffffffu;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const uint64_t sum = (uint64_t)l[e] + (e < 3 ? PX[e] : 0u) + c;
+            S[e] = (uint32_t)sum;
+            c = sum >> 32;
+            all &= S[e];
+        }
+        st = c ? 2 : (all == 0xffffffffu ? 1 : 0);
+    }
+    const ChainMasks cm = chain_prepare(st, sh.w);
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t c0 = chain_out(sh.w, 0u), c1 = chain_out(sh.w, 1u);
+        kinds[t] = c0 | (c1 << 1);
+    }
+    const uint32_t mc = chain_mine(cm, sh.w, 0u);
+    uint32_t w[E];
+    {
+        uint64_t c = mc;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const uint64_t sum = (uint64_t)S[e] + c;
+            w[e] = (uint32_t)sum;
+            c = sum >> 32;
+        }
+    }
+    if (j0 + E <= M && ((reinterpret_cast<uintptr_t>(out + j0) & 15u) == 0)) {
+        uint4* o = reinterpret_cast<uint4*>(out + j0);
+        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (j0 + e < M) out[j0 + e] = w[e];
+    }
+}
+
+// One CTA: the carry bit into every tile from the kinds k_garner_words left
+// (bit 0: carry out for carry-in 0, bit 1: for carry-in 1), then +1 at the
+// first word of every tile whose carry-in is 1, rippling inside the tile.
+// Each thread takes a contiguous run of tiles; a run passes on a constant
+// (its last non-propagating tile's carry) or its own carry-in, and a scan over
+// the runs in shared memory gives each run its carry-in.
+constexpr int kFixThreads = 1024;
+static __global__ void __launch_bounds__(kFixThreads)
+k_carry_fix(const uint32_t* __restrict__ kinds, uint32_t ntiles, uint32_t* __restrict__ out,
+            size_t M) {
+    __shared__ uint32_t s_f[kFixThreads];  // 0, 1: constant carry out; 2: passes carry-in
+    const int tid = threadIdx.x;
+    const uint32_t per = (ntiles + kFixThreads - 1) / kFixThreads;
+    const uint32_t t0 = min(ntiles, (uint32_t)tid * per), t1 = min(ntiles, t0 + per);
+    uint32_t f = 2;
+    for (uint32_t t = t0; t < t1; ++t) {
+        const uint32_t k = __ldcg(kinds + t);
+        if (k == 0u || k == 3u) f = k & 1u;  // kill / generate: a constant
+    }
+    s_f[tid] = f;
+    __syncthreads();
+    // inclusive scan of "the latest constant": combine(a, b) = b unless b
+    // passes its carry-in
+    for (int d = 1; d < kFixThreads; d <<= 1) {
+        const uint32_t a = tid >= d ? s_f[tid - d] : 2u;
+        __syncthreads();
+        if (s_f[tid] == 2u) s_f[tid] = a;
+        __syncthreads();
+    }
+    uint32_t eps = tid > 0 ? s_f[tid - 1] : 0u;
+    if (eps == 2u) eps = 0u;  // nothing before this run sets it: carry-in 0
+    for (uint32_t t = t0; t < t1; ++t) {
+        const uint32_t k = __ldcg(kinds + t);
+        if (eps) {
+            const size_t beg = (size_t)t * kCarryTileWords;
+            const size_t end = min(M, beg + kCarryTileWords);
+            if (k == 2u) {
+                // a propagating tile's words are all ones: with the carry in
+                // they all become zero (and the carry passes on)
+                for (size_t i = beg; i < end; ++i) out[i] = 0u;
+            } else {
+                for (size_t i = beg; i < end; ++i) {
+                    const uint32_t v = out[i] + 1u;
+                    out[i] = v;
+                    if (v != 0u) break;
+                }
+            }
+        }
+        eps = (k >> eps) & 1u;
     }
 }
 
@@ -1267,7 +1539,7 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
     const int log_n = P.log_n;
     const int n = 1 << log_n;
     T* bufA = reinterpret_cast<T*>(smem_raw);
-    T* bufB = bufA + n;
+    T* bufB = bufA + tile_elems(n);
     T* res = scratch + d.res_off;
     const size_t nca = (size_t)d.la * CPW, ncb = (size_t)d.lb * CPW;
     const int sq = d.square;
@@ -1280,7 +1552,7 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
             return (T)__ldg(src + i);
         }
     };
-    auto ldA = [&](int, int idx) -> T { return bufA[swz<T>(idx)]; };
+    auto ldA = [&](int, int, int p) -> T { return bufA[p]; };
 
     for (int kp = 0; kp < P.K; ++kp) {
         const PrimeDev<Ar>& pr = P.pr[kp];
@@ -1290,17 +1562,17 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
             res[(size_t)kp * n + idx] = ar.red1(ar.shoup(v, sc.w, sc.wq));
         };
         for (int i = threadIdx.x; i < n; i += NT) {
-            bufA[swz<T>(i)] = coef(d.a, nca, i);
-            if (!sq) bufB[swz<T>(i)] = coef(d.b, ncb, i);
+            bufA[LayRow::p(i)] = coef(d.a, nca, i);
+            if (!sq) bufB[LayRow::p(i)] = coef(d.b, ncb, i);
         }
         __syncthreads();
         for (int op = 0; op < (sq ? 1 : 2); ++op) {
             T* buf = op ? bufB : bufA;
             const int rounds = (op == 0 && !sq) ? nr : nr - 1;
-            auto ld = [&](int, int idx) -> T { return buf[swz<T>(idx)]; };
-            auto st = [&](int, int idx, T v) { buf[swz<T>(idx)] = v; };
+            auto ld = [&](int, int, int p) -> T { return buf[p]; };
+            auto st = [&](int, int, int p, T v) { buf[p] = v; };
             for (int r = 0; r < rounds; ++r) {
-                run_round_rl<Ar, RLOG, false, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
+                run_round_rl<Ar, LayRow, RLOG, false, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
                                                      sched_s0<RLOG>(log_n, r), pr.WCf, ar, false,
                                                      ld, st);
                 __syncthreads();
@@ -1318,21 +1590,20 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
                 const int j = sp & ((1 << d_log) - 1);
                 const int g = sp >> d_log;
                 const int base = (g << (d_log + rl)) + j;
+                const int p0 = LayRow::p(base);   // last round: stride 1 (d_log = 0)
                 T x[1 << RLOG];
 #define BW_SMALL_FUSED(RL)                                                             \
     {                                                                                  \
-        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] =                   \
-            src[swz<T>(base + (k << d_log))];                                          \
+        _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) x[k] = src[p0 + k];     \
         ct_stages<Ar, RL, false>(x, s0, g, pr.WCf, ar, false);                         \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
             const T xa = ar.fwd_to_2p(x[k]);                                           \
-            const T ya = sq ? xa : ar.fwd_to_2p(bufA[swz<T>(base + (k << d_log))]);    \
+            const T ya = sq ? xa : ar.fwd_to_2p(bufA[p0 + k]);                         \
             x[k] = ar.mont(xa, ya);                                                    \
         }                                                                              \
         gs_stages<Ar, RL, false>(x, s0, g, pr.WCi, ar);                                \
         _Pragma("unroll") for (int k = 0; k < (1 << RL); ++k) {                        \
-            const int idx = base + (k << d_log);                                       \
-            if (final_round) st_res(idx, x[k]); else bufA[swz<T>(idx)] = x[k];         \
+            if (final_round) st_res(base + k, x[k]); else bufA[p0 + k] = x[k];         \
         }                                                                              \
     }
                 if (rl == RLOG) {
@@ -1350,14 +1621,14 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
         }
         for (int r = nr - 2; r >= 0; --r) {
             const bool last = (r == 0);
-            auto st = [&](int, int idx, T v) {
+            auto st = [&](int, int idx, int p, T v) {
                 if (last) {
                     st_res(idx, v);
                 } else {
-                    bufA[swz<T>(idx)] = v;
+                    bufA[p] = v;
                 }
             };
-            run_round_rl<Ar, RLOG, true, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
+            run_round_rl<Ar, LayRow, RLOG, true, false>(sched_rl<RLOG>(log_n, r), log_n, 0,
                                                 sched_s0<RLOG>(log_n, r), pr.WCi, ar, false, ldA,
                                                 st);
             __syncthreads();
