@@ -82,15 +82,19 @@ struct Ar32 {
     }
 };
 
-// The 64-bit path's primes are p = c 2^32 + 1 with 2^61 <= p < 2^64 / 6 (62
-// bits).  Every multiplication by a constant inside and between the transforms
-// uses the truncated Shoup quotient, which omits the x0*v0 partial product (q
-// may be 2 short, so the product lies in [0, 3p)).  The forward (CT)
-// transform keeps values in [0, 6p + 2^32); its input reduction compares the
-// high word only (subtract 3p when hi > 3c).  The inverse (GS) transform keeps
-// values in [0, 3p): sums are reduced by one conditional subtraction of 3p,
-// differences are offset by 3p (6p < 2^64).  Garner and the final scalings
-// use the exact quotient.
+// The 64-bit path's primes are p = c 2^32 + 1 below 2^58, so 64p < 2^64.
+// Every multiplication by a constant inside and between the transforms uses
+// the truncated Shoup quotient, which omits the x0*v0 partial product (q may
+// be 2 short, so the product lies in [0, 3p)).  The forward (CT) butterfly
+// adds without reducing: from inputs below 3p its stage-0 sums stay below 6p
+// and every later stage adds less than 3p, so s stages stay below 3p (s + 1)
+// -- below 64p for the at most 13 stages one pass runs (the headroom the
+// 58-bit primes buy: with primes near 2^62 every butterfly reduced its input).
+// The inverse (GS) transform keeps values in [0, 3p): sums are reduced by one
+// conditional subtraction of 3p, differences are offset by 3p (6p < 2^64).
+// A forward output enters the pointwise product reduced to [0, 2p) by an
+// exact Shoup multiplication by 1.  Garner and the final scalings use the
+// exact quotient.
 struct Ar64 {
     using T = uint64_t;
     static constexpr int BITS = 64;
@@ -103,6 +107,7 @@ struct Ar64 {
     uint64_t p4;    // 4p
     uint64_t mu_lo; // floor(2^128 / p) = mu_hi 2^64 + mu_lo
     uint32_t mu_hi;
+    uint64_t oneq;  // floor(2^64 / p): Shoup companion of 1
 
     __device__ __forceinline__ T red2(T a) const { return min(a, a - p2); }
     __device__ __forceinline__ T red1(T a) const { return min(a, a - p); }
@@ -188,10 +193,11 @@ struct Ar64 {
             : "l"(x), "l"(w), "l"(wq), "r"(c));
         return r;
     }
-    // forward CT butterfly, inputs/outputs in [0, 6p + 2^32)
+    // forward CT butterfly: a + t and a - t + 3p with t = b w in [0, 3p), no
+    // reduction (each stage grows the bound by less than 3p)
     __device__ __forceinline__ void ct(T& a, T& b, T w, T wq) const {
-        const T x = ((uint32_t)(a >> 32) > c3) ? a - p3 : a;  // [0, 3p + 2^32)
-        const T t = shoup3(b, w, wq);                          // [0, 3p)
+        const T x = a;
+        const T t = shoup3(b, w, wq);  // [0, 3p)
         a = x + t;
         b = x - t + p3;
     }
@@ -213,8 +219,8 @@ struct Ar64 {
         a = min(u, u - p3);
         b = min(v, v - p3);
     }
-    // forward-transform output range [0, 6p + 2^32) -> [0, 2p)
-    __device__ __forceinline__ T fwd_to_2p(T a) const { return red2(min(a, a - p4)); }
+    // forward-transform output (any value below 2^64) -> [0, 2p)
+    __device__ __forceinline__ T fwd_to_2p(T a) const { return shoup(a, 1, oneq); }
     // inverse-transform output range [0, 3p) -> [0, p)
     __device__ __forceinline__ T inv_out(T a) const { return red1(min(a, a - p2)); }
     // x * w for a twiddle applied between transform passes, in [0, 3p)

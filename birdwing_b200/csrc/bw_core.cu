@@ -89,14 +89,16 @@ uint32_t bitrev_h(uint32_t x, int bits) {
 }
 
 // Primes of the two paths with a generator of the multiplicative group.
-// P64: c * 2^32 + 1, the largest such primes below 2^64 / 6 (62 bits,
-//      v2(p-1) = 32; the bound is what the forward butterfly's lazy range
-//      [0, 6p + 2^32) needs).
+// P64: c * 2^32 + 1, the largest such primes below 2^58 (v2(p-1) = 32): 64p
+//      fits in 64 bits, so a forward transform of up to 20 stages adds its
+//      butterflies' sums without reducing them (values stay below 3p (s + 1)
+//      after s stages); three of them (2^174) still carry 64-bit
+//      coefficients, whose convolution stays below 2^160.
 // P32: primes below 2^30 with v2(p-1) = 26, 25, 24: the first two (K = 2)
 //      allow transforms of 2^25 points, and their product (2^56.1) bounds
 //      every product of that length (min(L_A, L_B) (2^16 - 1)^2 < p0 p1).
-const uint64_t kP64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
-const uint64_t kG64[3] = {10, 7, 3};
+const uint64_t kP64[3] = {0x3ffffd500000001ull, 0x3ffffcf00000001ull, 0x3ffffa500000001ull};
+const uint64_t kG64[3] = {5, 11, 7};
 const uint64_t kP32[3] = {469762049ull, 167772161ull, 754974721ull};
 const uint64_t kG32[3] = {3, 3, 11};
 
@@ -171,6 +173,7 @@ inline void set_c(Ar64& a, uint64_t p) {
     const u128 mu = (~(u128)0) / p;  // floor(2^128 / p): p is odd
     a.mu_lo = (uint64_t)mu;
     a.mu_hi = (uint32_t)(mu >> 64);
+    a.oneq = (uint64_t)(((u128)1 << 64) / p);
 }
 
 template <class Ar>

@@ -475,9 +475,9 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                     if (zt && idx >= R / 2) return T(0);
                     T x = PP ? buf[p] : (T)coef[(idx << log_cb) + v];
                     if constexpr (W64) {
-                        // 2^64 < 6.0001 p: two conditional 3p steps reach [0, 3p)
-                        x = min(x, x - ar.p3);
-                        x = min(x, x - ar.p3);
+                        // a 64-bit coefficient (up to 64p) enters reduced to
+                        // [0, 2p), leaving the transform its headroom
+                        x = ar.fwd_to_2p(x);
                     }
                     return x;
                 }

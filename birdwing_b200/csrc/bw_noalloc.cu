@@ -102,6 +102,7 @@ void garner_constants(int path, int K, int log_n, PlanDev<Ar>& pd) {
             const u128 mu = (~(u128)0) / p;
             pr.ar.mu_lo = (uint64_t)mu;
             pr.ar.mu_hi = (uint32_t)(mu >> 64);
+            pr.ar.oneq = (uint64_t)(((u128)1 << 64) / p);
         }
         pr.one_q = (T)companion(1, p, bits);
     }

@@ -13,11 +13,11 @@
 
 // RNS tables of this width: libbirdwing's primes with maximal-order roots.
 #if LIMB_BITS == 64 && defined(NATIVE_HOST_LIMBS)
-vector<TestDataTypeUint> moduli = {0x2aaaaa9500000001ULL, 0x2aaaaa8f00000001ULL,
-                                   0x2aaaaa6f00000001ULL};
+vector<TestDataTypeUint> moduli = {0x3ffffd500000001ULL, 0x3ffffcf00000001ULL,
+                                   0x3ffffa500000001ULL};
 vector<TestDataTypeUint> roots_of_unity_max = {0, 0, 0};
 #elif LIMB_BITS == 64
-vector<TestDataTypeUint> moduli = {0x2aaaaa9500000001ULL, 0x2aaaaa8f00000001ULL};
+vector<TestDataTypeUint> moduli = {0x3ffffd500000001ULL, 0x3ffffcf00000001ULL};
 vector<TestDataTypeUint> roots_of_unity_max = {0, 0};
 #else
 vector<TestDataTypeUint> moduli = {469762049u, 167772161u, 754974721u};
@@ -26,7 +26,7 @@ vector<TestDataTypeUint> roots_of_unity_max = {0, 0, 0};
 
 namespace {
 
-// the path the lifecycle drives: 62-bit primes (u32 coefficients); the CRT
+// the path the lifecycle drives: 58-bit primes (u32 coefficients); the CRT
 // coefficients it can dump are then those of the limb-level convolution
 constexpr int kPath = BW_PATH_P64;
 constexpr int kWordsPerLimb = INPUT_LIMB_BITS / 32;
@@ -48,9 +48,9 @@ uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
 // generator of the multiplicative group of each library prime
 uint64_t generator(uint64_t p) {
     switch (p) {
-        case 0x2aaaaa9500000001ULL: return 10;
-        case 0x2aaaaa8f00000001ULL: return 7;
-        case 0x2aaaaa6f00000001ULL: return 3;
+        case 0x3ffffd500000001ULL: return 5;
+        case 0x3ffffcf00000001ULL: return 11;
+        case 0x3ffffa500000001ULL: return 7;
         case 754974721u: return 11;
         case 469762049u: return 3;
         case 167772161u: return 3;

@@ -398,8 +398,8 @@ done:
 
 /* The library's two bases (same primes as libbirdwing), roots derived from a
  * generator of the multiplicative group. */
-static const uint64_t P64[3] = {0x2aaaaa9500000001ull, 0x2aaaaa8f00000001ull, 0x2aaaaa6f00000001ull};
-static const uint64_t G64[3] = {10, 7, 3};
+static const uint64_t P64[3] = {0x3ffffd500000001ull, 0x3ffffcf00000001ull, 0x3ffffa500000001ull};
+static const uint64_t G64[3] = {5, 11, 7};
 static const uint64_t P32[3] = {469762049ull, 167772161ull, 754974721ull};
 static const uint64_t G32[3] = {3, 3, 11};
 
@@ -416,7 +416,7 @@ int oracle_path_basis(int path, uint64_t* primes, uint64_t* roots_max, int* max_
 }
 
 /* path 32: 16-bit coefficients over the 30-bit primes; path 64: 32-bit
- * coefficients over the 62-bit primes. */
+ * coefficients over the 58-bit primes. */
 int oracle_multiply(int path, int K, const uint32_t* a, size_t la, const uint32_t* b, size_t lb,
                     uint32_t* out) {
     uint64_t primes[3], roots[3];
