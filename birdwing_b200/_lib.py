@@ -35,6 +35,9 @@ BW_PLAN_WIDE_COLS = 1 << 19
 BW_PLAN_COEF64 = 1 << 20
 BW_PLAN_RADIX16 = 1 << 21
 BW_PLAN_COL_RADIX8 = 1 << 22
+BW_PLAN_TMA_COLS = 1 << 23
+BW_PLAN_NO_TMA_COLS = 1 << 24
+BW_PLAN_SHFL_ROWS = 1 << 25
 
 BW_BATCH_THREE_PRIMES = 1
 BW_BATCH_UPLOAD = 1

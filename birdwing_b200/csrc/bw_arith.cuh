@@ -221,6 +221,13 @@ struct Ar64 {
     }
     // forward-transform output (any value below 2^64) -> [0, 2p)
     __device__ __forceinline__ T fwd_to_2p(T a) const { return shoup(a, 1, oneq); }
+    // a 64-bit coefficient -> [0, 2p): the path's primes are c 2^32 + 1 with
+    // 2^25 < c < 2^26, so q = x >> 58 is floor(x / p) or one less (x / p - q
+    // < 1 + 2^-13), and x - q p = (x - q) - (q c) 2^32
+    __device__ __forceinline__ T reduce_in(T x) const {
+        const uint32_t q = (uint32_t)(x >> 58);
+        return x - q - ((uint64_t)(q * c) << 32);
+    }
     // inverse-transform output range [0, 3p) -> [0, p)
     __device__ __forceinline__ T inv_out(T a) const { return red1(min(a, a - p2)); }
     // x * w for a twiddle applied between transform passes, in [0, 3p)

@@ -221,11 +221,21 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
     const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
     const size_t smem2 = ntab * sizeof(Tw<T>) + tile_elems(C) * sizeof(T) * 2;
     const dim3 g2(R, pl.K, np);
-    switch (std::min(512, std::max(64, C >> 4))) {
-        case 512: kb_row<Ar, 512, 4><<<g2, 512, smem2, s>>>(P, g.d_desc, ra, rb); break;
-        case 256: kb_row<Ar, 256, 4><<<g2, 256, smem2, s>>>(P, g.d_desc, ra, rb); break;
-        case 128: kb_row<Ar, 128, 4><<<g2, 128, smem2, s>>>(P, g.d_desc, ra, rb); break;
-        default: kb_row<Ar, 64, 4><<<g2, 64, smem2, s>>>(P, g.d_desc, ra, rb); break;
+    if constexpr (sizeof(T) == 8) {
+        // radix-8 rounds on at most 256 threads (64 registers, as the
+        // single-product row pass of the 64-bit path)
+        switch (std::min(256, std::max(64, C >> 3))) {
+            case 256: kb_row<Ar, 256, 3><<<g2, 256, smem2, s>>>(P, g.d_desc, ra, rb); break;
+            case 128: kb_row<Ar, 128, 3><<<g2, 128, smem2, s>>>(P, g.d_desc, ra, rb); break;
+            default: kb_row<Ar, 64, 3><<<g2, 64, smem2, s>>>(P, g.d_desc, ra, rb); break;
+        }
+    } else {
+        switch (std::min(512, std::max(64, C >> 4))) {
+            case 512: kb_row<Ar, 512, 4><<<g2, 512, smem2, s>>>(P, g.d_desc, ra, rb); break;
+            case 256: kb_row<Ar, 256, 4><<<g2, 256, smem2, s>>>(P, g.d_desc, ra, rb); break;
+            case 128: kb_row<Ar, 128, 4><<<g2, 128, smem2, s>>>(P, g.d_desc, ra, rb); break;
+            default: kb_row<Ar, 64, 4><<<g2, 64, smem2, s>>>(P, g.d_desc, ra, rb); break;
+        }
     }
     const size_t smem3 = tile_elems((size_t)R * CB) * sizeof(T);
     kb_inv_col<Ar, 4><<<dim3(C / CB, pl.K, np), kColThreads, smem3, s>>>(P, g.d_desc, ra);
@@ -252,8 +262,8 @@ int set_group_attrs() {
         set((const void*)kb_fwd_col<Ar32, true, 4>);
         set((const void*)kb_inv_col<Ar64, 4>);
         set((const void*)kb_inv_col<Ar32, 4>);
-        for (auto f : {(const void*)kb_row<Ar64, 64, 4>, (const void*)kb_row<Ar64, 128, 4>,
-                       (const void*)kb_row<Ar64, 256, 4>, (const void*)kb_row<Ar64, 512, 4>,
+        for (auto f : {(const void*)kb_row<Ar64, 64, 3>, (const void*)kb_row<Ar64, 128, 3>,
+                       (const void*)kb_row<Ar64, 256, 3>,
                        (const void*)kb_row<Ar32, 64, 4>, (const void*)kb_row<Ar32, 128, 4>,
                        (const void*)kb_row<Ar32, 256, 4>, (const void*)kb_row<Ar32, 512, 4>})
             set(f);

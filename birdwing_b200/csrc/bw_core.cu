@@ -425,6 +425,8 @@ static unsigned sm_count() {
     return (unsigned)n;
 }
 
+constexpr int kTmaColsMinLogN = 20;
+
 int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int mode) {
     pl->path = path;
     pl->K = K;
@@ -526,6 +528,21 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
                        : (flags & BW_PLAN_RADIX16) ? 4
                        : r8_default                ? 3
                                                    : 4;
+        // inverse column tiles by tensor copies: single products with two
+        // passes, from 2^20 points unless forced either way (a box is at most
+        // 256 columns wide and 16 bytes or more).  Measured at 2^23 words:
+        // the inverse pass 0.246 -> 0.231 ms (64-bit coefficients), 0.378 ->
+        // 0.348 ms (32-bit path); at 2^17 points 0.016 -> 0.018 ms.
+        const bool tma_want = (flags & BW_PLAN_TMA_COLS) ||
+                              (!(flags & BW_PLAN_NO_TMA_COLS) && log_n >= kTmaColsMinLogN);
+        pl->tma_cols = (tma_want && mode == 2 && pl->log_r2 == 0 && !pl->tw_smem_r &&
+                        pl->log_cb <= 8 && (w << pl->log_cb) >= 16)
+                           ? 1
+                           : 0;
+        pl->shfl_rows = ((flags & BW_PLAN_SHFL_ROWS) && mode == 2 && path == BW_PATH_P32 &&
+                         pl->log_c == 12 && pl->rlog_row == 4)
+                            ? 1
+                            : 0;
         pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
         pl->lo_out = (log_n + 1) / 2;
     }
@@ -656,7 +673,46 @@ struct bw_ctx {
     size_t out_tiles_per = 0;      // carry tiles per K4 launch
     int spin_limit = 1 << 22;
     bool inject_wait_fault = false;
+    CUtensorMap tmap_res;          // residues of A as [prime][row][column] (tma_cols)
 };
+
+// Tensor map of a context's A residues for the TMA form of the inverse column
+// pass: dims (columns, rows, primes), boxes of CB columns x min(R, 256) rows.
+// cuTensorMapEncodeTiled comes from the driver through the runtime's entry
+// point query, so the library needs no link to libcuda.
+static int encode_residue_map(bw_ctx* c) {
+    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<EncodeFn>(fn);
+    });
+    if (!encode) return bw_fail(BW_ECUDA, "cuTensorMapEncodeTiled is not available");
+    const bw_plan* pl = c->plan;
+    const int w = pl->path == BW_PATH_P64 ? 8 : 4;
+    const cuuint64_t C = (cuuint64_t)1 << pl->log_c, R = (cuuint64_t)1 << pl->log_r;
+    const cuuint64_t dims[3] = {C, R, (cuuint64_t)pl->K};
+    const cuuint64_t strides[2] = {C * w, C * R * w};
+    const cuuint32_t box[3] = {1u << pl->log_cb, (cuuint32_t)std::min<cuuint64_t>(R, 256), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (((cuuint64_t)box[0] * w) % 16 != 0)
+        return bw_fail(BW_EINVAL, "column tile of %u x %d bytes is not a 16-byte multiple", box[0], w);
+    const CUresult r = encode(&c->tmap_res,
+                              w == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+                              3, c->d_res_a, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return bw_fail(BW_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return BW_OK;
+}
 
 extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
     bw_clear_error();
@@ -707,6 +763,10 @@ extern "C" int bw_ctx_create(bw_ctx** out, const bw_plan* pl, void* stream) {
     for (auto& ev : c->stage_ev)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
             return fail(bw_fail(BW_ECUDA, "event: %s", cudaGetErrorString(e)));
+    if (pl->tma_cols) {
+        const int rc = encode_residue_map(c);
+        if (rc) return fail(rc);
+    }
     if (pl->order) {
         std::lock_guard<std::mutex> lk(pl->order->mu);
         pl->order->contexts++;
@@ -840,8 +900,10 @@ int set_smem_attrs() {
         set((const void*)k_row<Ar, 128, 3>);
         set((const void*)k_row<Ar, 256, 3>);
         set((const void*)k_row<Ar, 512, 3>);
+        if constexpr (sizeof(typename Ar::T) == 4) set((const void*)k_row<Ar, 256, 4, true>);
         set((const void*)k_mid_col<Ar, false>);
         set((const void*)k_mid_col<Ar, true>);
+        set((const void*)k_inv_col_tma<Ar, 4>);
         if constexpr (sizeof(typename Ar::T) == 8) {
             set((const void*)k_fwd_col<Ar, SPLIT16, 3, true, false, true>);
             set((const void*)k_fwd_col<Ar, SPLIT16, 3, false, false, true>);
@@ -880,6 +942,12 @@ void launch_row(const bw_plan* pl, const PlanDev<Ar>& pd, typename Ar::T* ra,
     // CTA per SM at 70 registers)
     const int cap = (RLOG == 3 || sizeof(typename Ar::T) == 4) ? 256 : 512;
     const int want = std::min(cap, std::max(64, 1 << (pl->log_c - RLOG)));
+    if constexpr (sizeof(typename Ar::T) == 4 && RLOG == 4) {
+        if (pl->shfl_rows && want == 256) {
+            k_row<Ar, 256, 4, true><<<g, 256, smem, s>>>(pd, ra, rb, sq);
+            return;
+        }
+    }
     switch (want) {
         case 512: k_row<Ar, 512, RLOG><<<g, 512, smem, s>>>(pd, ra, rb, sq); break;
         case 256: k_row<Ar, 256, RLOG><<<g, 256, smem, s>>>(pd, ra, rb, sq); break;
@@ -1079,8 +1147,13 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
     const size_t smem3 = tw_bytes + tile_elems((size_t)R * CB) * sizeof(T);
     dim3 g3(cols_outer / CB, pl->K);
     bool inv_done = false;
+    if (pl->tma_cols) {
+        k_inv_col_tma<Ar, 4><<<g3, kColThreads, (size_t)R * CB * sizeof(T) + 128, c->stream>>>(
+            pd, ra, c->cst, c->tmap_res, c->err, c->spin_limit);
+        inv_done = true;
+    }
     if constexpr (PP) {
-        if (pl->rlog_col == 3) {
+        if (!inv_done && pl->rlog_col == 3) {
             if (ts) {
                 k_inv_col<Ar, 3, true><<<g3, kColThreads, smem3, c->stream>>>(pd, ra, c->cst);
             } else {

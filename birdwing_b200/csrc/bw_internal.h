@@ -32,6 +32,8 @@ struct bw_plan {
     int log_cb2 = 0, lo_out = 0;
     int small = 0;       // single-pass plan: the whole n-point transform in one CTA
     int w64 = 0;         // 64-bit path with 64-bit coefficients (two words each, K = 3)
+    int tma_cols = 0;    // inverse column tiles by tensor copies (BW_PLAN_TMA_COLS)
+    int shfl_rows = 0;   // row pass exchange through warp shuffles (BW_PLAN_SHFL_ROWS)
     int device = 0;
     bool zt_a = false, zt_b = false;
     void* d_tables = nullptr;

@@ -34,6 +34,8 @@
 // (src/gpu_ntt.cu:216-238), crt_combine_kernel (src/crt_gpu.cu:157-276) and the
 // three carry kernels (src/carry_prop.cu:8-211).
 #pragma once
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded on the host)
+
 #include <cstdint>
 #include <type_traits>
 #include "bw_arith.cuh"
@@ -411,6 +413,22 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                                           : 0u);
             }
         }
+    } else if (W64 && PP && (reinterpret_cast<uintptr_t>(limbs) & 7u) == 0) {
+        // 64-bit coefficients of an 8-byte-aligned operand: one 8-byte copy
+        // each into the residue tile (a lone last word: 4 bytes, high word 0)
+        for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
+            const size_t wi = 2 * ((size_t)(e >> log_cb) * C + c0 + (e & (CB - 1)));
+            T* dst = buf + LayCol<T>::p(e);
+            if (wi + 1 < ncoef) {
+                cp_async_elem(dst, reinterpret_cast<const T*>(limbs + wi));
+            } else if (wi < ncoef) {
+                uint32_t* d32 = reinterpret_cast<uint32_t*>(dst);
+                cp_async_elem(d32, limbs + wi);
+                d32[1] = 0;
+            } else {
+                *dst = 0;
+            }
+        }
     } else {
         for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
             const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
@@ -477,7 +495,7 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                     if constexpr (W64) {
                         // a 64-bit coefficient (up to 64p) enters reduced to
                         // [0, 2p), leaving the transform its headroom
-                        x = ar.fwd_to_2p(x);
+                        x = ar.reduce_in(x);
                     }
                     return x;
                 }
@@ -537,6 +555,23 @@ kb_fwd_col(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
 }
 
 // ------------------------------------------------------------------ K2
+// One stage of a 16 x 16 register transpose across the 16 lanes of a
+// half-warp (four stages, SH = 1, 2, 4, 8): for every register pair (k, k|SH)
+// the lane whose bit SH is clear keeps x[k] and trades x[k|SH] for its
+// partner's x[k]; the partner trades x[k] for this lane's x[k|SH].
+template <int SH, typename T>
+__device__ __forceinline__ void shfl_transpose_step(T (&x)[16], int lane) {
+    const bool up = (lane & SH) != 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & SH) continue;
+        const T send = up ? x[k] : x[k | SH];
+        const T recv = __shfl_xor_sync(0xffffffffu, send, SH);
+        x[k] = up ? recv : x[k];
+        x[k | SH] = up ? x[k | SH] : recv;
+    }
+}
+
 // Per-row twiddle tables: F[i] = w^(i k1), G[j] = w^(j 2^a k1) (forward) and
 // the inverse pair with n^-1 2^bits folded into Gi.  w^e comes from the
 // plan's two-level tables; each entry's Shoup companion is computed here.
@@ -555,7 +590,7 @@ __device__ __forceinline__ Tw<typename Ar::T> pow_entry(const Ar& ar, uint64_t e
 // on load, forward C-point NTT of both rows, pointwise product, inverse
 // C-point NTT, inverse twiddle.  The result overwrites the A row.
 // square: B is A.
-template <class Ar, int NT, int RLOG>
+template <class Ar, int NT, int RLOG, bool SHFL = false>
 __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* res_a,
                                          const typename Ar::T* res_b, int square, int prow,
                                          int kp, unsigned char* smem_raw) {
@@ -612,11 +647,19 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
         ga[idx] = ar.mulc(ar.mulc(v, f.w, f.wq), g.w, g.wq);
     };
 
+    // the warp-shuffle exchange (BW_PLAN_SHFL_ROWS): 2^12-point rows of the
+    // 32-bit path on 256 threads, one radix-16 sub-problem per thread per
+    // round; B's stride-16 round hands its outputs to the fused stride-1
+    // round through registers (a 16 x 16 transpose inside each half-warp)
+    // instead of shared memory
+    constexpr bool kShflShape = SHFL && sizeof(T) == 4 && RLOG == 4 && NT == 256;
+    const bool shfl = kShflShape && log_c == 12 && !square;
+
     // forward rounds: A fully (all but the last when squaring), B all but the
     // last (its last round is fused with the product below)
     for (int op = 0; op < (square ? 1 : 2); ++op) {
         T* buf = op ? bufB : bufA;
-        const int rounds = (op == 0 && !square) ? nr : nr - 1;
+        const int rounds = (op == 0 && !square) ? nr : nr - 1 - (op == 1 && shfl ? 1 : 0);
         auto ld = [&](int, int, int p) -> T { return buf[p]; };
         auto st = [&](int, int, int p, T v) { buf[p] = v; };
         for (int r = 0; r < rounds; ++r) {
@@ -627,11 +670,42 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
         }
     }
 
+    if constexpr (kShflShape) {
+        if (shfl) {
+            // B's stride-16 round (stages 4-7) from shared memory ...
+            const int tid = threadIdx.x, lane = tid & 15, g = tid >> 4;
+            const int s_mid = sched_s0<4>(log_c, nr - 2), s_last = sched_s0<4>(log_c, nr - 1);
+            const int base = (g << 8) + lane;
+            const int p0 = LayRow::p(base), S = LayRow::stride(4);
+            T x[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = bufB[p0 + k * S];
+            ct_stages<Ar, 4, false>(x, s_mid, g, pr.WCf, ar, false);
+            // ... then lane j' of the half-warp takes element 16 j' + m of
+            // the group's 256 (held by lane m as its register j')
+            shfl_transpose_step<1>(x, lane);
+            shfl_transpose_step<2>(x, lane);
+            shfl_transpose_step<4>(x, lane);
+            shfl_transpose_step<8>(x, lane);
+            // the fused round on sub-problem tid (stride 1): stages 8-11,
+            // product with A, first inverse stages
+            const int pb = LayRow::p(tid << 4);
+            ct_stages<Ar, 4, false>(x, s_last, tid, pr.WCf, ar, false);
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                x[k] = ar.mont(ar.fwd_to_2p(x[k]), ar.fwd_to_2p(bufA[pb + k]));
+            gs_stages<Ar, 4, false>(x, s_last, tid, pr.WCi, ar);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) bufA[pb + k] = x[k];
+            __syncthreads();
+        }
+    }
+
     // fused round: last forward round of B (or A), pointwise product, first
     // inverse round -- one sub-problem stays in registers throughout.  The
     // last round of the schedule has stride 1 (d_log = 0), so the slots of a
     // sub-problem are swz(base) + k.
-    {
+    if (!shfl) {
         const int r = nr - 1;
         const int rl = sched_rl<RLOG>(log_c, r), s0 = sched_s0<RLOG>(log_c, r);
         const int d_log = log_c - s0 - rl;
@@ -688,11 +762,11 @@ __device__ __forceinline__ void row_body(const PlanDev<Ar>& P, typename Ar::T* r
     }
 }
 
-template <class Ar, int NT, int RLOG>
+template <class Ar, int NT, int RLOG, bool SHFL = false>
 __global__ void __launch_bounds__(NT)
 k_row(const PlanDev<Ar> P, typename Ar::T* res_a, const typename Ar::T* res_b, int square) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    row_body<Ar, NT, RLOG>(P, res_a, res_b, square, blockIdx.x, blockIdx.y, smem_raw);
+    row_body<Ar, NT, RLOG, SHFL>(P, res_a, res_b, square, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 // batched: blockIdx.z = product
@@ -845,6 +919,111 @@ __device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::
         };
         run_round_rl<Ar, LayCol<T>, RLOG, true, TS>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
                                          sched_s0<RLOG>(log_r, r), W, ar, false, ld, st);
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ K3, TMA form
+// The inverse column pass with its tile brought in by the tensor-memory
+// accelerator (BW_PLAN_TMA_COLS): one thread issues R / BR box copies
+// (cp.async.bulk.tensor.3d, CB columns x BR rows of prime blockIdx.y, no
+// multicast) that complete on a shared-memory mbarrier; every thread waits on
+// it (bounded).  A tensor copy writes its box densely, so the rounds run on an
+// unpadded tile (its stride-CB first round has bank conflicts the padded
+// layouts avoid); it is the measured alternative to the per-element cp.async
+// of k_inv_col.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <class Ar, int RLOG>
+__global__ void __launch_bounds__(kColThreads)
+k_inv_col_tma(const PlanDev<Ar> P, typename Ar::T* res, CarryState* cst,
+              const __grid_constant__ CUtensorMap tmap, uint32_t* __restrict__ err,
+              int spin_limit) {
+    using T = typename Ar::T;
+    using L = Lay<4, 0>;  // dense, as the tensor copies write it
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_ok;
+    const int tile = blockIdx.x, kp = blockIdx.y;
+    if (tile == 0 && kp == 0 && threadIdx.x == 0) cst->counter = 0;
+    const int log_r = P.log_r, log_c = P.log_c, log_cb = P.log_cb;
+    const int R = 1 << log_r, CB = 1 << log_cb;
+    const size_t C = (size_t)1 << log_c;
+    const size_t n = (size_t)R * C;
+    const int c0 = tile << log_cb;
+    const PrimeDev<Ar>& pr = P.pr[kp];
+    const Ar ar = pr.ar;
+    T* g = res + (size_t)kp * n;
+    // tensor copies land on 128-byte-aligned shared addresses (the launch
+    // gives 128 bytes of slack)
+    T* buf = reinterpret_cast<T*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
+    const int BR = R < 256 ? R : 256;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_ok = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bar, (unsigned)((size_t)R * CB * sizeof(T)));
+        for (int i = 0; i < R / BR; ++i)
+            tma_load_3d(buf + (size_t)i * BR * CB, &tmap, c0, i * BR, kp, &bar);
+    }
+    {
+        int it = 0;
+        while (!mbar_try_wait(&bar, 0u)) {
+            if (++it > spin_limit) {
+                s_ok = 0;
+                atomicOr(err, 1u);
+                break;
+            }
+        }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const int nr = sched_rounds<RLOG>(log_r);
+    for (int r = nr - 1; r >= 0; --r) {
+        const bool last = (r == 0);
+        auto ld = [&](int, int, int p) -> T { return buf[p]; };
+        auto st = [&](int v, int idx, int p, T val) {
+            if (last) {
+                g[(size_t)idx * C + c0 + v] = ar.inv_out(val);
+            } else {
+                buf[p] = val;
+            }
+        };
+        run_round_rl<Ar, L, RLOG, true, false>(sched_rl<RLOG>(log_r, r), log_r, log_cb,
+                                               sched_s0<RLOG>(log_r, r), pr.WRi, ar, false, ld, st);
         __syncthreads();
     }
 }
@@ -1522,12 +1701,20 @@ kb_garner_carry(const PlanDev<Ar> P, const BatchProd* __restrict__ D,
 // global scratch (L2-resident at these sizes); then Garner + carry over the
 // product's words in tiles of NT*8 words, the carry handed from tile to tile
 // inside the CTA, so no look-back is needed.
+// Register bounds: 64-bit residues run radix-8 rounds in 64 registers (four
+// 256-thread CTAs per SM; radix 16 took 128, two per SM, 12.5% warps
+// active); 32-bit residues get at most 128 (unbounded they took 185, one
+// 256-thread CTA per SM).
+template <class Ar>
+constexpr int ks_min_blocks(int nt) {
+    return sizeof(typename Ar::T) == 8 ? 1024 / nt : 512 / nt;
+}
 template <class Ar, bool SPLIT16, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, ks_min_blocks<Ar>(NT))
 ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* scratch,
            uint32_t* __restrict__ err) {
     using T = typename Ar::T;
-    constexpr int RLOG = 4;
+    constexpr int RLOG = sizeof(T) == 8 ? 3 : 4;
     constexpr int E = kCarryWordsPerThread;
     constexpr int CPW = SPLIT16 ? 2 : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];

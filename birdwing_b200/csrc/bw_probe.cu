@@ -20,6 +20,8 @@ using namespace bw;
 
 namespace {
 
+using u128 = unsigned __int128;
+
 template <class Ar>
 struct ProbeArgs {
     Ar ar;
@@ -66,8 +68,6 @@ k_bfly_rate(const ProbeArgs<Ar> P, int iters, typename Ar::T* out) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
 }
 
-using u128 = unsigned __int128;
-
 uint64_t companion(uint64_t w, uint64_t p, int bits) {
     return bits == 64 ? (uint64_t)(((u128)w << 64) / p) : (uint64_t)((w << 32) / p);
 }
@@ -85,6 +85,7 @@ int run_probe(int iters, int ctas_per_sm, float* ms, double* butterflies) {
         P.ar.c3 = 3u * P.ar.c;
         P.ar.p3 = 3 * p;
         P.ar.p4 = 4 * p;
+        P.ar.oneq = (uint64_t)(((u128)1 << 64) / p);
     }
     for (int l = 0; l < 4; ++l) {
         const uint64_t w = (0x1234567u * (l + 3)) % p;

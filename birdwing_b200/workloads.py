@@ -114,6 +114,13 @@ PLAIN = {
         expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=21),
         ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
         desc="plain 2^26-bit x 2^26-bit product (profiling size)"),
+    # the same size on the 32-bit path (16-bit coefficients, two primes)
+    "prof32": dict(
+        words_a=1 << 21, words_b=1 << 21, seeds=(1234, 5678), square=False,
+        plan=(BW_PATH_P32, 2, 0),
+        expect=dict(path=32, coeff_bits=16, num_primes=2, log_n=23, log_cols=12),
+        ref=(32, 2), literal=(BW_PATH_P32, 2, 0),
+        desc="plain 2^26-bit x 2^26-bit product on the 32-bit path (profiling size)"),
 }
 
 

@@ -96,6 +96,19 @@ extern "C" {
 #define BW_PLAN_RADIX16     (1u << 21)
 /* Radix-8 rounds in the column passes (single products on the 64-bit path). */
 #define BW_PLAN_COL_RADIX8  (1u << 22)
+/* Single products, two-pass schedule: the inverse column pass brings its tile
+ * into shared memory with tensor-memory-accelerator box copies
+ * (cp.async.bulk.tensor, one mbarrier) instead of per-element cp.async, and
+ * runs its rounds on the dense tile.  On by default from transforms of 2^20
+ * points (measured faster there, slower below); BW_PLAN_TMA_COLS forces it
+ * on, BW_PLAN_NO_TMA_COLS off. */
+#define BW_PLAN_TMA_COLS    (1u << 23)
+#define BW_PLAN_NO_TMA_COLS (1u << 24)
+/* Single products on the 32-bit path with 2^12-point rows: the row pass hands
+ * one round's outputs to the next through warp shuffles (a 16 x 16 transpose
+ * inside each half-warp) instead of shared memory.  A measured alternative,
+ * off by default. */
+#define BW_PLAN_SHFL_ROWS   (1u << 25)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):

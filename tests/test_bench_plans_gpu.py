@@ -48,7 +48,7 @@ def plans_of(name):
     return ["plan"] + (["literal"] if w["literal"] != w["plan"] else [])
 
 
-@pytest.mark.parametrize("name,which", [(n, k) for n in ("1", "2", "2sq", "prof")
+@pytest.mark.parametrize("name,which", [(n, k) for n in ("1", "2", "2sq", "prof", "prof32")
                                         for k in plans_of(n)])
 def test_benchmarked_plan_bit_exact(name, which):
     w = workloads.PLAIN[name]

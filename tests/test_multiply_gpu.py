@@ -624,6 +624,55 @@ def test_radix_switches_exact():
                     assert (c.multiply(a, b) == want).all(), (la, lb, K, sw)
 
 
+def test_tma_inverse_columns_exact():
+    """The inverse column pass with tensor-copy tiles (BW_PLAN_TMA_COLS) and
+    with per-element cp.async (BW_PLAN_NO_TMA_COLS) give the same exact
+    products on both paths, for every coefficient width, squarings and
+    device pointers at an odd word offset (graph replay)."""
+    import torch
+    L = bw._lib
+    rng = np.random.default_rng(71)
+    for la, lb in [(1, 1), (3000, 1777), (65537, 4097), ((1 << 19) + 3, (1 << 18) - 5)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = gmp_ref.mul(a, b)
+        for path, K in ((64, 0), (64, 2), (32, 2), (32, 3)):
+            for fl in (L.BW_PLAN_TMA_COLS, L.BW_PLAN_NO_TMA_COLS):
+                with bw.Plan(la, lb, path, K, flags=fl) as p, bw.Context(p) as c:
+                    assert (c.multiply(a, b) == want).all(), (la, lb, path, K, fl)
+                    if la == lb:
+                        assert (c.square(a) == gmp_ref.mul(a, a)).all()
+    # device pointers, the operand at an odd word offset, graph replay twice
+    la = lb = (1 << 20) + 1
+    a, b = rand_words(la, rng), rand_words(lb, rng)
+    want = gmp_ref.mul(a, b)
+    buf = torch.from_numpy(np.concatenate([[7], a, b]).astype(np.uint32).view(np.int32)).cuda()
+    dc = torch.empty(la + lb, dtype=torch.int32, device="cuda")
+    for fl in (L.BW_PLAN_TMA_COLS, L.BW_PLAN_NO_TMA_COLS):
+        with bw.Plan(la, lb, 64, 0, flags=fl) as p, bw.Context(p) as c:
+            for _ in range(2):
+                dc.fill_(-1)
+                c.multiply_device(buf.data_ptr() + 4, la, buf.data_ptr() + 4 * (1 + la), lb,
+                                  dc.data_ptr(), la + lb)
+                c.sync()
+                assert (dc.cpu().numpy().view(np.uint32) == want).all(), fl
+
+
+def test_shuffle_row_exchange_exact():
+    """The warp-shuffle exchange of the 32-bit path's 2^12-point rows
+    (BW_PLAN_SHFL_ROWS) gives the products of the shared-memory exchange;
+    squarings keep the shared-memory path."""
+    L = bw._lib
+    rng = np.random.default_rng(73)
+    for la, lb in [((1 << 21) - 7, (1 << 21) + 5), (1 << 22, (1 << 21) + 1), (1 << 21, 1 << 21)]:
+        a, b = rand_words(la, rng), rand_words(lb, rng)
+        want = gmp_ref.mul(a, b)
+        with bw.Plan(la, lb, 32, 2, flags=L.BW_PLAN_SHFL_ROWS) as p, bw.Context(p) as c:
+            assert p.info["log_cols"] == 12
+            assert (c.multiply(a, b) == want).all(), (la, lb)
+            if la == lb:
+                assert (c.square(a) == gmp_ref.mul(a, a)).all()
+
+
 @pytest.mark.gpu
 def test_coef64_squaring_chunks_and_ring():
     """64-bit coefficients: squarings through every chunk count, and products
