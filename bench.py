@@ -2,7 +2,8 @@
 
 Default workload (configuration 2): one plain 2^28-bit x 2^28-bit product
 (2^23 u32 words each, uniform random with the top bit set, seeded), 32-bit
-coefficients, n = 2^24, two 62-bit primes (64-bit prime path).  A "step" is
+coefficients, n = 2^24, two 58-bit primes (64-bit prime path); the library's
+plan for it runs 64-bit coefficients over three primes.  A "step" is
 one full product.  Metric: products/s (whole job), with the per-stage times,
 the HBM roofline of the dominant kernel and the product-level algorithmic
 byte model (12*K*n*w + in + out) beside it.
@@ -59,7 +60,7 @@ def ref_algorithm(cfg):
     cpw = 2 if path == 32 else 1
     log_n = max(4, ((la + (la if square else lb)) * cpw - 2).bit_length())
     return (f"reference algorithm: {32 // cpw}-bit coefficients, n=2^{log_n}, {K} x "
-            f"{62 if path == 64 else 30}-bit primes (CPU restatement)")
+            f"{58 if path == 64 else 30}-bit primes (CPU restatement)")
 
 
 # batched configurations: (products, seed, K, description)

@@ -1,9 +1,10 @@
 // bw_arith.cuh -- exact modular arithmetic for the two prime paths.
 //
-// Residues are kept lazily reduced (Harvey): the forward Cooley-Tukey
-// butterfly keeps values in [0, 4p), the inverse Gentleman-Sande butterfly in
-// [0, 2p).  Both need 4p < 2^bits, which is why the 32-bit path uses primes
-// below 2^30 and the 64-bit path primes below 2^62.
+// Residues are kept lazily reduced (Harvey).  On the 32-bit path the forward
+// Cooley-Tukey butterfly keeps values in [0, 4p) and the inverse
+// Gentleman-Sande butterfly in [0, 2p), which needs 4p < 2^32 (primes below
+// 2^30).  The 64-bit path's primes are below 2^58, which leaves its forward
+// transform 64x headroom (see Ar64).
 //
 // Multiplication by a precomputed constant w uses Shoup's method with the
 // companion wq = floor(w * 2^bits / p): q = hi(x * wq), r = x*w - q*p lies in

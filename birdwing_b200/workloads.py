@@ -135,6 +135,6 @@ def plain_plan_args(name, which="plan"):
 
 def algorithm_of(info):
     """One-line description of what a plan runs, from bw_plan_info fields."""
-    prime_bits = 62 if info["path"] == 64 else 30
+    prime_bits = 58 if info["path"] == 64 else 30
     return (f"{info['coeff_bits']}-bit coefficients, n=2^{info['log_n']}, "
             f"{info['num_primes']} x {prime_bits}-bit primes ({info['path']}-bit prime path)")

@@ -14,7 +14,7 @@
  *   BW_PATH_P32 : 16-bit coefficients, 30-bit primes, 32-bit modular
  *                 arithmetic (the reference's LIMB_BITS=32 pipeline, whose
  *                 transform length is twice the limb count).
- *   BW_PATH_P64 : 32-bit coefficients, 62-bit primes of the form c*2^32+1,
+ *   BW_PATH_P64 : 32-bit coefficients, 58-bit primes of the form c*2^32+1,
  *                 64-bit modular arithmetic (the reference's LIMB_BITS=64
  *                 "hybrid" and NATIVE_HOST_LIMBS pipelines; a u64 limb array
  *                 is passed as twice as many u32 words).

@@ -16,7 +16,7 @@
  *
  * Garner follows crt_combine_many (src/crt.cpp:42-87) and the mixed-radix
  * kernel (src/crt_gpu.cu:157-276), with the running value kept in three
- * 64-bit words so that three 62-bit primes fit.  Carry propagation follows
+ * 64-bit words so that three 64-bit-path primes fit.  Carry propagation follows
  * the serial reference of tests/test_carry_prop.cu:20-35 / scripts/carry.py.
  * The schoolbook product follows tests/test_full_multiply.cpp:27-58.
  *
