@@ -89,10 +89,11 @@ def parse():
 def parse_args_list(argv):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS))
+    ap.add_argument("--config", default="2",
+                    choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS) + ["intpeak"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--autotune", action="store_true",
@@ -107,6 +108,9 @@ def parse_args_list(argv):
                     help="4-step split override (BW_PLAN_LOG_COLS), 0 = automatic")
     ap.add_argument("--plan-flags", type=lambda s: int(s, 0), default=0,
                     help="extra bw_plan_create flags (tuning switches)")
+    ap.add_argument("--persistent", action="store_true",
+                    help="batched configurations: small buckets as one persistent kernel per "
+                         "path over a device work queue (BW_BATCH_PERSISTENT)")
     ap.add_argument("--no-sub", action="store_true",
                     help="plain configuration 2: skip the batched and serving sub-records")
     return ap.parse_args(argv)
@@ -499,7 +503,7 @@ def bench_batch(args):
         ha = torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)
         hb = torch.from_numpy(b.view(np.int32)).pin_memory().numpy().view(np.uint32)
         pinned.append((p, ha, hb))
-    bt = bw.Batch(num_primes=K, stream=stream.cuda_stream)
+    bt = bw.Batch(num_primes=K, stream=stream.cuda_stream, persistent=args.persistent)
     outs = [bt.add(a, b, path=p) for p, a, b in pinned]
     if args.autotune:
         bt.autotune(reps=3)
@@ -596,7 +600,7 @@ def bench_batch(args):
         peak, peak_kind = load_peaks()
         mb = batch_model_bytes(items, K)
         achieved = mb / (ms * 1e-3) / 1e9
-        launches = info["small_buckets"] + 4 * (info["buckets"] - info["small_buckets"])
+        launches = info["kernel_nodes"]
         h2d = sum(4 * (len(a) + len(b)) for _, a, b in items)
         d2h = sum(4 * (len(a) + len(b)) for _, a, b in items) + 4
         line = {
@@ -609,6 +613,8 @@ def bench_batch(args):
                        "small_buckets": info["small_buckets"],
                        "graph_nodes": info["graph_nodes"],
                        "device_bytes": info["device_bytes"], "autotuned": bool(args.autotune),
+                       "small_form": "persistent queue kernel per path" if args.persistent
+                                     else "graph of per-bucket grids",
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "correct_vs_gmp": ok,
@@ -934,8 +940,60 @@ def run_reference_serving(args):
     print(json.dumps(line))
 
 
+def bench_intpeak(args):
+    """Integer-pipe ceiling of both prime paths (bw_butterfly_rate): the
+    transforms' own forward and inverse butterflies from registers, no memory
+    traffic, swept over 2/4/8 CTAs of 256 threads per SM, best of 3 each.
+    Reported per second and per SM-cycle at the SM clock sampled during the
+    timed launches; the plain configurations' int_floor divides their
+    butterflies by the same rate."""
+    import torch
+
+    from birdwing_b200 import _lib as L
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no integer-throughput probe: its transforms "
+                          "are the absent GPU-NTT library's"}))
+        return
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.05)
+    paths, t0 = {}, time.perf_counter()
+    for name, path in (("p32", L.BW_PATH_P32), ("p64", L.BW_PATH_P64)):
+        best, sweep = butterfly_rate(path)
+        paths[name] = {"butterflies_per_s": best,
+                       "ctas_per_sm": max(sweep, key=sweep.get),
+                       "sweep": {str(c): r for c, r in sweep.items()}}
+    t1 = time.perf_counter()
+    clocks.region(t0, t1)
+    ck = clocks.stop()
+    mhz = ck.get("sm_mhz") or 0.0
+    for v in paths.values():
+        v["per_sm_cycle"] = v["butterflies_per_s"] / (sms * mhz * 1e6) if mhz else None
+    line = {
+        "metric": "butterflies/s", "value": paths["p64"]["butterflies_per_s"],
+        "unit": "butterflies/s", "n_gpus": 1, "steps": 3, "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "intpeak: 16 residues per thread, two radix-16 forward rounds "
+                               "and one inverse round per iteration (96 butterflies), 2000 "
+                               "iterations, 256-thread CTAs",
+                   "sms": sms},
+        "paths": paths, "p32_over_p64": paths["p32"]["butterflies_per_s"]
+        / paths["p64"]["butterflies_per_s"],
+        "gpu_launches": 2 * 3 * 3 * 2, "clocks": ck,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.config == "intpeak":
+        bench_intpeak(args)
+        return
     if args.config in SERVE_CONFIGS:
         if args.impl == "reference":
             run_reference_serving(args)
@@ -987,17 +1045,21 @@ def plan_butterflies(info, square):
 
 def butterfly_rate(path, iters=2000):
     """Integer-pipe ceiling of the path's butterflies (bw_butterfly_rate):
-    butterflies per second with nothing else running, best of 3."""
+    butterflies per second with nothing else running, best of 3 at each of
+    2/4/8 CTAs per SM.  Returns (best rate, {ctas_per_sm: rate})."""
     import ctypes
 
     from birdwing_b200 import _lib as L
-    best = None
-    for _ in range(3):
-        ms, bf = ctypes.c_float(), ctypes.c_double()
-        L.check(L.lib.bw_butterfly_rate(path, iters, 4, ctypes.byref(ms), ctypes.byref(bf)))
-        r = bf.value / (ms.value * 1e-3)
-        best = r if best is None else max(best, r)
-    return best
+    sweep = {}
+    for cps in (2, 4, 8):
+        best = None
+        for _ in range(3):
+            ms, bf = ctypes.c_float(), ctypes.c_double()
+            L.check(L.lib.bw_butterfly_rate(path, iters, cps, ctypes.byref(ms), ctypes.byref(bf)))
+            r = bf.value / (ms.value * 1e-3)
+            best = r if best is None else max(best, r)
+        sweep[cps] = best
+    return max(sweep.values()), sweep
 
 
 def run_sub_bench(extra, timeout):
@@ -1290,13 +1352,14 @@ def bench_plain(args):
         if world == 1:
             # integer-pipe floor: the plan's butterflies at the rate the
             # path's butterflies reach with nothing else running
-            rate = butterfly_rate(path)
+            rate, _ = butterfly_rate(path)
             bfly = plan_butterflies(info, square)
             floor_ms = bfly / rate * 1e3
             line["int_floor"] = {"butterflies": bfly, "butterflies_per_s": rate,
                                  "floor_ms": floor_ms, "frac": floor_ms / ms,
                                  "how": "bw_butterfly_rate: the path's own forward and inverse "
-                                        "butterflies from registers on 4 CTAs per SM, best of 3"}
+                                        "butterflies from registers, best over 2/4/8 CTAs per SM "
+                                        "(bench.py --config intpeak)"}
             line["int_floor_frac"] = floor_ms / ms
         if not args.no_cpu_baseline and world == 1:   # the CPU baseline runs at N = 1 only
             line["cpu_baseline"] = cpu_baseline(cfg)

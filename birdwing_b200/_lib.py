@@ -40,6 +40,7 @@ BW_PLAN_NO_TMA_COLS = 1 << 24
 BW_PLAN_SHFL_ROWS = 1 << 25
 
 BW_BATCH_THREE_PRIMES = 1
+BW_BATCH_PERSISTENT = 2
 BW_BATCH_UPLOAD = 1
 BW_BATCH_COMPUTE = 2
 BW_BATCH_DOWNLOAD = 4
@@ -84,7 +85,8 @@ class bw_limits_info(ctypes.Structure):
 
 class bw_batch_info(ctypes.Structure):
     _fields_ = [(n, ctypes.c_size_t) for n in
-                ("products", "buckets", "small_buckets", "graph_nodes", "device_bytes")]
+                ("products", "buckets", "small_buckets", "graph_nodes", "device_bytes",
+                 "kernel_nodes")]
 
 
 class bw_server_config(ctypes.Structure):

@@ -259,9 +259,11 @@ class Batch:
     host_multiply_merge call per product.
     """
 
-    def __init__(self, num_primes=2, stream=None):
+    def __init__(self, num_primes=2, stream=None, persistent=False):
         h = ctypes.c_void_p()
         flags = L.BW_BATCH_THREE_PRIMES if num_primes == 3 else 0
+        if persistent:
+            flags |= L.BW_BATCH_PERSISTENT
         check(lib.bw_batch_create(ctypes.byref(h), ctypes.c_void_p(stream or 0), flags))
         self._h = h
         self._keep = []

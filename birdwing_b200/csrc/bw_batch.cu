@@ -71,6 +71,9 @@ constexpr int kSmallDefaultLog = 12;
 // Products per bucket: kb_fwd_col puts 2 * products in gridDim.z (<= 65535).
 constexpr size_t kMaxBucket = 16384;
 
+// Threads of the persistent small-product kernel (BW_BATCH_PERSISTENT).
+constexpr int kQueueThreads = 256;
+
 TuneVal tune_get(int path, int K, int log_n) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(TuneKey{path, K, log_n});
@@ -160,13 +163,34 @@ struct bw_batch {
     cudaEvent_t ev[4] = {};
     cudaEvent_t chunk_ev[kStageChunks] = {};
     size_t graph_nodes = 0;
+    size_t kernel_nodes = 0;
     int spin_limit = 1 << 22;
     bool inject_wait_fault = false;
+    // BW_BATCH_PERSISTENT: per prime path (0: 64-bit, 1: 32-bit), the small
+    // buckets' device table, their work items and the queue head
+    bool persistent = false;
+    void* d_qbuckets[2] = {};
+    SmallItem* d_qitems[2] = {};
+    uint32_t* d_qhead = nullptr;  // two counters
+    uint32_t qcount[2] = {0, 0};
+    int qlog_max[2] = {0, 0};
 };
 
 namespace {
 
+void drop_queues(bw_batch* bt) {
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(bt->d_qbuckets[i]);
+        cudaFree(bt->d_qitems[i]);
+        bt->d_qbuckets[i] = nullptr;
+        bt->d_qitems[i] = nullptr;
+        bt->qcount[i] = 0;
+        bt->qlog_max[i] = 0;
+    }
+}
+
 void drop_layout(bw_batch* bt) {
+    drop_queues(bt);
     if (bt->exec) cudaGraphExecDestroy(bt->exec);
     if (bt->graph) cudaGraphDestroy(bt->graph);
     bt->exec = nullptr;
@@ -258,6 +282,8 @@ int set_group_attrs() {
         set((const void*)ks_product<Ar32, true, 64>);
         set((const void*)ks_product<Ar32, true, 128>);
         set((const void*)ks_product<Ar32, true, 256>);
+        set((const void*)kq_small<Ar64, false, kQueueThreads>);
+        set((const void*)kq_small<Ar32, true, kQueueThreads>);
         set((const void*)kb_fwd_col<Ar64, false, 4>);
         set((const void*)kb_fwd_col<Ar32, true, 4>);
         set((const void*)kb_inv_col<Ar64, 4>);
@@ -307,6 +333,56 @@ void bw_group_fill_state(bw::BatchProd& d, unsigned char* state, size_t ntiles) 
 }
 
 namespace {
+
+// BW_BATCH_PERSISTENT: the device table of one path's small buckets and its
+// work items, largest transforms first.
+template <class Ar>
+int upload_queue(bw_batch* bt, int slot, const std::vector<size_t>& sb) {
+    std::vector<SmallBucketDev<Ar>> tab(sb.size());
+    std::vector<SmallItem> items;
+    int log_max = 0;
+    for (size_t j = 0; j < sb.size(); ++j) {
+        const Bucket& bk = bt->buckets[sb[j]];
+        tab[j].plan = pdev<Ar>(bk.plan);
+        tab[j].desc = bk.d_desc;
+        tab[j].scratch = static_cast<typename Ar::T*>(bk.d_res_a);
+        log_max = std::max(log_max, bk.log_n);
+        for (size_t q = 0; q < bk.prods.size(); ++q)
+            items.push_back(SmallItem{(uint32_t)j, (uint32_t)q});
+    }
+    std::stable_sort(items.begin(), items.end(), [&](const SmallItem& x, const SmallItem& y) {
+        return bt->buckets[sb[x.bucket]].log_n > bt->buckets[sb[y.bucket]].log_n;
+    });
+    BW_TRY(cudaMalloc(&bt->d_qbuckets[slot], tab.size() * sizeof(SmallBucketDev<Ar>)));
+    BW_TRY(cudaMemcpy(bt->d_qbuckets[slot], tab.data(), tab.size() * sizeof(SmallBucketDev<Ar>),
+                      cudaMemcpyHostToDevice));
+    BW_TRY(cudaMalloc(&bt->d_qitems[slot], items.size() * sizeof(SmallItem)));
+    BW_TRY(cudaMemcpy(bt->d_qitems[slot], items.data(), items.size() * sizeof(SmallItem),
+                      cudaMemcpyHostToDevice));
+    bt->qcount[slot] = (uint32_t)items.size();
+    bt->qlog_max[slot] = log_max;
+    return BW_OK;
+}
+
+// One path's queue kernel: as many CTAs as fit on the SMs at the largest
+// transform's shared memory.
+template <class Ar, bool SPLIT16>
+cudaError_t launch_queue(bw_batch* bt, int slot, cudaStream_t s) {
+    using T = typename Ar::T;
+    const size_t smem = 2 * tile_elems((size_t)1 << bt->qlog_max[slot]) * sizeof(T);
+    auto kern = kq_small<Ar, SPLIT16, kQueueThreads>;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kQueueThreads, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const unsigned grid = (unsigned)std::min<size_t>((size_t)std::max(per_sm, 1) * sms,
+                                                     bt->qcount[slot]);
+    kern<<<grid, kQueueThreads, smem, s>>>(
+        static_cast<const SmallBucketDev<Ar>*>(bt->d_qbuckets[slot]), bt->d_qitems[slot],
+        bt->qcount[slot], bt->d_qhead + slot, bt->d_err);
+    return cudaGetLastError();
+}
 
 // Build (or rebuild) buckets, arenas, descriptors and the graph.
 int build_layout(bw_batch* bt) {
@@ -410,6 +486,19 @@ int build_layout(bw_batch* bt) {
         BW_TRY(cudaMalloc(&bk.d_desc, np * sizeof(BatchProd)));
         BW_TRY(cudaMemcpy(bk.d_desc, desc.data(), np * sizeof(BatchProd), cudaMemcpyHostToDevice));
     }
+    // persistent form: one work queue per path over its small buckets
+    if (bt->persistent) {
+        if (!bt->d_qhead) BW_TRY(cudaMalloc(&bt->d_qhead, 2 * sizeof(uint32_t)));
+        for (int slot = 0; slot < 2; ++slot) {
+            const int path = slot == 0 ? BW_PATH_P64 : BW_PATH_P32;
+            std::vector<size_t> sb;
+            for (size_t i = 0; i < bt->buckets.size(); ++i)
+                if (bt->buckets[i].small && bt->buckets[i].path == path) sb.push_back(i);
+            if (sb.empty()) continue;
+            rc = slot == 0 ? upload_queue<Ar64>(bt, slot, sb) : upload_queue<Ar32>(bt, slot, sb);
+            if (rc) return rc;
+        }
+    }
     // graph: clear look-back state and the error word, then every bucket on
     // its own branch
     BW_TRY(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
@@ -418,6 +507,7 @@ int build_layout(bw_batch* bt) {
         if (ce == cudaSuccess) ce = e;
     };
     chk(cudaMemsetAsync(bt->d_err, 0, 4, bt->stream));
+    if (bt->persistent) chk(cudaMemsetAsync(bt->d_qhead, 0, 2 * sizeof(uint32_t), bt->stream));
     for (const Bucket& bk : bt->buckets) {
         if (bk.d_state) {
             chk(cudaMemsetAsync(bk.d_state, 0, bk.prods.size() * bw_group_state_stride(bk.ntiles),
@@ -435,12 +525,25 @@ int build_layout(bw_batch* bt) {
         const auto& b = bt->buckets[y];
         return (a.prods.size() << a.log_n) > (b.prods.size() << b.log_n);
     });
+    // the persistent queues first (one branch per path), then the other
+    // buckets round-robin after them
+    size_t branch = 0;
+    if (bt->persistent) {
+        rc = set_group_attrs();
+        for (int slot = 0; slot < 2 && rc == BW_OK; ++slot) {
+            if (!bt->qcount[slot]) continue;
+            chk(slot == 0 ? launch_queue<Ar64, false>(bt, slot, bt->side[branch % nside])
+                          : launch_queue<Ar32, true>(bt, slot, bt->side[branch % nside]));
+            ++branch;
+        }
+    }
     for (size_t i = 0; i < order.size() && rc == BW_OK; ++i) {
         const Bucket& bk = bt->buckets[order[i]];
+        if (bt->persistent && bk.small) continue;
         bw_group_launch g{&bk.plan, bk.d_desc, (unsigned)bk.prods.size(), bk.d_res_a,
                           bk.d_res_b, bk.ntiles, bt->d_err, bt->spin_limit,
                           bt->inject_wait_fault};
-        rc = bw_enqueue_group(g, bt->side[i % nside]);
+        rc = bw_enqueue_group(g, bt->side[branch++ % nside]);
     }
     for (int s = 0; s < nside; ++s) {
         chk(cudaEventRecord(bt->join[s], bt->side[s]));
@@ -455,6 +558,15 @@ int build_layout(bw_batch* bt) {
     size_t nodes = 0;
     cudaGraphGetNodes(bt->graph, nullptr, &nodes);
     bt->graph_nodes = nodes;
+    std::vector<cudaGraphNode_t> all(nodes);
+    bt->kernel_nodes = 0;
+    if (nodes && cudaGraphGetNodes(bt->graph, all.data(), &nodes) == cudaSuccess) {
+        for (size_t i = 0; i < nodes; ++i) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(all[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+                bt->kernel_nodes++;
+        }
+    }
     bt->dirty = false;
     return BW_OK;
 }
@@ -473,6 +585,7 @@ extern "C" int bw_batch_create(bw_batch** out, void* stream, unsigned flags) {
     *out = nullptr;
     bw_batch* bt = new bw_batch();
     bt->K = (flags & BW_BATCH_THREE_PRIMES) ? 3 : 2;
+    bt->persistent = (flags & BW_BATCH_PERSISTENT) != 0;
     auto fail = [&](int rc) {
         bw_batch_destroy(bt);
         return rc;
@@ -509,6 +622,7 @@ extern "C" int bw_batch_destroy(bw_batch* bt) {
     cudaFreeHost(bt->h_in);
     cudaFreeHost(bt->h_out);
     cudaFree(bt->d_err);
+    cudaFree(bt->d_qhead);
     cudaFreeHost(bt->h_err);
     for (int s = 0; s < bw_batch::kSide; ++s) {
         if (bt->side[s]) cudaStreamDestroy(bt->side[s]);
@@ -654,6 +768,7 @@ extern "C" int bw_batch_get_info(const bw_batch* bt, bw_batch_info* o) {
     o->products = bt->prods.size();
     o->buckets = bt->buckets.size();
     o->graph_nodes = bt->graph_nodes;
+    o->kernel_nodes = bt->kernel_nodes;
     size_t bytes = (bt->in_cap + bt->out_cap) * 4;
     for (const Bucket& b : bt->buckets) {
         const size_t n = (size_t)1 << b.log_n;

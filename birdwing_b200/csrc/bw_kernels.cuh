@@ -1710,19 +1710,18 @@ constexpr int ks_min_blocks(int nt) {
     return sizeof(typename Ar::T) == 8 ? 1024 / nt : 512 / nt;
 }
 template <class Ar, bool SPLIT16, int NT>
-__global__ void __launch_bounds__(NT, ks_min_blocks<Ar>(NT))
-ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* scratch,
-           uint32_t* __restrict__ err) {
+__device__ __forceinline__ void ks_product_body(const PlanDev<Ar>& P, const BatchProd& d,
+                                                typename Ar::T* scratch,
+                                                uint32_t* __restrict__ err,
+                                                unsigned char* smem_raw) {
     using T = typename Ar::T;
     constexpr int RLOG = sizeof(T) == 8 ? 3 : 4;
     constexpr int E = kCarryWordsPerThread;
     constexpr int CPW = SPLIT16 ? 2 : 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_w[NT / 32];
     __shared__ uint32_t s_lastx[NT / 32][3];
     __shared__ uint32_t s_cin[3];
     __shared__ uint32_t s_eps;
-    const BatchProd d = D[blockIdx.x];
     const int log_n = P.log_n;
     const int n = 1 << log_n;
     T* bufA = reinterpret_cast<T*>(smem_raw);
@@ -1901,6 +1900,48 @@ ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T*
         __syncthreads();
     }
     if (bad) atomicOr(err, 2u);
+}
+
+template <class Ar, bool SPLIT16, int NT>
+__global__ void __launch_bounds__(NT, ks_min_blocks<Ar>(NT))
+ks_product(const PlanDev<Ar> P, const BatchProd* __restrict__ D, typename Ar::T* scratch,
+           uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ks_product_body<Ar, SPLIT16, NT>(P, D[blockIdx.x], scratch, err, smem_raw);
+}
+
+// Persistent form of the small buckets of one prime path
+// (BW_BATCH_PERSISTENT): a grid of a few CTAs per SM pulls work items --
+// (bucket, product) pairs, largest transforms first -- from a device queue
+// (an atomic head) and runs each as ks_product does, reading the bucket's
+// plan and descriptor from device arrays.  The queue head is cleared before
+// every run; a CTA stops at the first item past the end.  No waits.
+struct SmallItem {
+    uint32_t bucket;
+    uint32_t prod;
+};
+template <class Ar>
+struct SmallBucketDev {
+    PlanDev<Ar> plan;
+    const BatchProd* desc;
+    typename Ar::T* scratch;
+};
+template <class Ar, bool SPLIT16, int NT>
+__global__ void __launch_bounds__(NT, ks_min_blocks<Ar>(NT))
+kq_small(const SmallBucketDev<Ar>* __restrict__ buckets, const SmallItem* __restrict__ items,
+         uint32_t count, uint32_t* __restrict__ head, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(head, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= count) break;
+        const SmallItem w = items[it];
+        const SmallBucketDev<Ar>& b = buckets[w.bucket];
+        ks_product_body<Ar, SPLIT16, NT>(b.plan, b.desc[w.prod], b.scratch, err, smem_raw);
+        __syncthreads();  // every thread has read s_item and left the body
+    }
 }
 
 }  // namespace bw

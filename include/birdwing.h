@@ -336,6 +336,12 @@ int bw_host_once_cache_limit(size_t bytes);
 typedef struct bw_batch bw_batch;
 
 #define BW_BATCH_THREE_PRIMES 1u  /* bw_batch_create: K = 3 (redundant check) */
+/* bw_batch_create: the small buckets (one CTA per product) of each prime path
+ * run as one persistent kernel that pulls (bucket, product) work items,
+ * largest transforms first, from a device queue, instead of one grid per
+ * bucket.  The other buckets are unchanged.  A measured alternative to the
+ * default graph of per-bucket grids. */
+#define BW_BATCH_PERSISTENT 2u
 
 /* bw_batch_run `what` bits (0 = all three) */
 #define BW_BATCH_UPLOAD 1u    /* copy every product's operands to the device */
@@ -348,6 +354,7 @@ typedef struct {
     size_t small_buckets;  /* groups run one CTA per product */
     size_t graph_nodes;    /* nodes of the captured graph */
     size_t device_bytes;   /* device memory the batch holds */
+    size_t kernel_nodes;   /* kernel launches per run (the graph's kernel nodes) */
 } bw_batch_info;
 
 /* stream = NULL creates a private stream. */

@@ -225,3 +225,45 @@ def test_lookback_wait_fault_is_reported_and_recoverable():
         bt.run()
         for (p, a, b), got in zip(items, outs):
             assert (got == gmp_ref.mul(a, b)).all()
+
+
+@pytest.mark.parametrize("K", [2, 3])
+def test_persistent_small_products_exact(K):
+    """BW_BATCH_PERSISTENT: the small buckets of both paths run as one
+    persistent kernel per path pulling work items from a device queue; every
+    product of a mixed batch (small and 4-step buckets, squarings) is
+    bit-exact against GMP, on the first run and on graph replays."""
+    rng = np.random.default_rng(41 + K)
+    items = []
+    for path in (64, 32):
+        for la, lb in [(1, 1), (2, 1), (7, 9), (64, 64), (100, 13), (511, 512), (1000, 999),
+                       (2047, 5), (3000, 3000), (20000, 7000)]:
+            a = rand_words(la, rng)
+            items.append((path, a, a if la == 64 else rand_words(lb, rng)))
+    with bw.Batch(num_primes=K, persistent=True) as bt:
+        outs = [bt.add(a, b, path=p) for p, a, b in items]
+        for rep in range(3):
+            for o in outs:
+                o[:] = 0
+            bt.run()
+            for (p, a, b), got in zip(items, outs):
+                assert (got == gmp_ref.mul(a, b)).all(), (rep, p, len(a), len(b))
+        info = bt.info()
+    assert info["small_buckets"] >= 2 and info["buckets"] > info["small_buckets"]
+
+
+def test_persistent_matches_graph_of_grids_on_the_mix():
+    """The benchmark's uneven mix (512 products) gives the same outputs in the
+    persistent form and in the default graph of per-bucket grids."""
+    items = workloads.batch_mix(512, seed=9)
+    res = {}
+    for persistent in (False, True):
+        with bw.Batch(num_primes=2, persistent=persistent) as bt:
+            outs = [bt.add(a, b, path=p) for p, a, b in items]
+            bt.run()
+            res[persistent] = [o.copy() for o in outs]
+    for x, y, (p, a, b) in zip(res[False], res[True], items):
+        assert (x == y).all()
+    for j in range(0, len(items), 37):
+        _, a, b = items[j]
+        assert (res[True][j] == gmp_ref.mul(a, b)).all()
