@@ -1273,25 +1273,37 @@ def bench_plain(args):
     # the workload as the reference states it (its coefficient width and
     # prime count), when the library's own plan differs: same operands, same
     # timing, rank 0 of a single-GPU run
-    literal = None
-    lp = plain_plan_args(cfg, "literal")
-    if world == 1 and PLAIN[cfg]["literal"] != PLAIN[cfg]["plan"]:
-        with bw.Plan(*lp[:4], flags=lp[4]) as lplan, bw.Context(lplan) as lctx:
-            lst = torch.cuda.ExternalStream(lctx.stream)
-            lstep = make_step(lctx)
+    def side_record(which):
+        """The same product under another plan of the table (same operands,
+        same timing): the workload as the reference states it, or the other
+        prime path."""
+        sp = plain_plan_args(cfg, which)
+        with bw.Plan(*sp[:4], flags=sp[4]) as splan, bw.Context(splan) as sctx:
+            sst = torch.cuda.ExternalStream(sctx.stream)
+            sstep = make_step(sctx)
             for _ in range(3):
-                lstep(False)
-            lctx.sync()
-            lok, _ = check_product()
-            lper = timed_products(lctx, lst, max(args.steps, 20))
-            lstage = stage_means(lctx, lst, 5)
-            lctx.sync()
-            li = lplan.info
-            literal = {"algorithm": algorithm_of(li), "coeff_bits": li["coeff_bits"],
-                       "num_primes": li["num_primes"], "log_n": li["log_n"],
-                       "ms_per_step": sum(lper) / len(lper),
-                       "value": len(lper) / (sum(lper) * 1e-3), "unit": "products/s",
-                       "stage_ms": lstage, "correct_vs_gmp": lok}
+                sstep(False)
+            sctx.sync()
+            sok, _ = check_product()
+            sper = timed_products(sctx, sst, max(args.steps, 20))
+            sstage = stage_means(sctx, sst, 5)
+            sctx.sync()
+            si = splan.info
+            return {"algorithm": algorithm_of(si), "path": si["path"],
+                    "coeff_bits": si["coeff_bits"], "num_primes": si["num_primes"],
+                    "log_n": si["log_n"], "ms_per_step": sum(sper) / len(sper),
+                    "value": len(sper) / (sum(sper) * 1e-3), "unit": "products/s",
+                    "stage_ms": sstage, "correct_vs_gmp": sok, "_info": si}
+
+    literal = None
+    if world == 1 and PLAIN[cfg]["literal"] != PLAIN[cfg]["plan"]:
+        literal = side_record("literal")
+        literal.pop("_info")
+    # the other prime path for the same product (the 32-bit path with 64-bit
+    # coefficients for the 2^28-bit workloads)
+    other = None
+    if world == 1 and PLAIN[cfg].get("other"):
+        other = side_record("other")
 
     if rank == 0:
         ms = total_ms / args.steps
@@ -1349,6 +1361,15 @@ def bench_plain(args):
         if literal:
             literal["product_roofline_frac"] = fixed / (literal["ms_per_step"] * 1e-3) / 1e9 / peak
             line["literal_config"] = literal
+        if other:
+            oi = other.pop("_info")
+            other["product_roofline_frac"] = fixed / (other["ms_per_step"] * 1e-3) / 1e9 / peak
+            orate, _ = butterfly_rate(oi["path"])
+            ofloor = plan_butterflies(oi, square) / orate * 1e3
+            other["int_floor"] = {"butterflies": plan_butterflies(oi, square),
+                                  "butterflies_per_s": orate, "floor_ms": ofloor}
+            other["int_floor_frac"] = ofloor / other["ms_per_step"]
+            line["other_path"] = other
         if world == 1:
             # integer-pipe floor: the plan's butterflies at the rate the
             # path's butterflies reach with nothing else running

@@ -38,6 +38,7 @@ BW_PLAN_COL_RADIX8 = 1 << 22
 BW_PLAN_TMA_COLS = 1 << 23
 BW_PLAN_NO_TMA_COLS = 1 << 24
 BW_PLAN_SHFL_ROWS = 1 << 25
+BW_PLAN_K1_ONE_PRIME = 1 << 26
 
 BW_BATCH_THREE_PRIMES = 1
 BW_BATCH_PERSISTENT = 2
@@ -74,7 +75,7 @@ class bw_plan_info(ctypes.Structure):
         ("log_rows", ctypes.c_int), ("log_cols", ctypes.c_int), ("coeff_bits", ctypes.c_int),
         ("la", ctypes.c_size_t), ("lb", ctypes.c_size_t), ("lc", ctypes.c_size_t),
         ("plan_device_bytes", ctypes.c_size_t), ("ctx_device_bytes", ctypes.c_size_t),
-        ("primes", ctypes.c_uint64 * 3),
+        ("primes", ctypes.c_uint64 * 6),
     ]
 
 

@@ -32,6 +32,9 @@ struct Ar32 {
     uint32_t p;
     uint32_t p2;    // 2p
     uint32_t pinv;  // -p^-1 mod 2^32
+    uint32_t r32;   // 2^32 mod p
+    uint32_t r32q;  // Shoup companion of r32
+    uint32_t oneq;  // floor(2^32 / p): Shoup companion of 1
 
     __device__ __forceinline__ T red2(T a) const { return min(a, a - p2); }
     __device__ __forceinline__ T red1(T a) const { return min(a, a - p); }
@@ -80,6 +83,13 @@ struct Ar32 {
     // Shoup companion floor(w 2^32 / p) of w < p
     __device__ __forceinline__ T companion(T w) const {
         return (uint32_t)((((uint64_t)w) << 32) / p);
+    }
+    // a 64-bit coefficient x = h 2^32 + l reduced to [0, 2p): h (2^32 mod p)
+    // and l * 1 by Shoup, each in [0, 2p), their sum below 4p
+    __device__ __forceinline__ T reduce64(uint64_t x) const {
+        const T h = shoup((uint32_t)(x >> 32), r32, r32q);
+        const T l = shoup((uint32_t)x, 1u, oneq);
+        return red2(h + l);
     }
 };
 

@@ -101,6 +101,13 @@ const uint64_t kP64[3] = {0x3ffffd500000001ull, 0x3ffffcf00000001ull, 0x3ffffa50
 const uint64_t kG64[3] = {5, 11, 7};
 const uint64_t kP32[3] = {469762049ull, 167772161ull, 754974721ull};
 const uint64_t kG32[3] = {3, 3, 11};
+// P32 with 64-bit coefficients: the six primes below 2^30 with v2(p-1) >= 23
+// and the largest residues, in ascending order (garner6_words_at relies on
+// it): transforms of up to 2^23 points, and a product of 2^177 against the
+// 2^150 bound of 2^22 coefficients of 64 bits (min(na, nb) 2^128).
+const uint64_t kP32W[6] = {595591169ull, 645922817ull, 754974721ull,
+                           880803841ull, 897581057ull, 998244353ull};
+const uint64_t kG32W[6] = {3, 3, 11, 26, 3, 3};
 
 int v2(uint64_t x) {
     int k = 0;
@@ -124,6 +131,15 @@ int bw_path_max_log_n(int path, int K) {
 }
 
 const uint64_t* bw_path_primes(int path) { return path == BW_PATH_P64 ? kP64 : kP32; }
+
+// The prime set of a plan and its generators: the path's own, or the six
+// 32-bit primes when the 32-bit path carries 64-bit coefficients.
+static const uint64_t* plan_primes(int path, bool w64) {
+    return (w64 && path == BW_PATH_P32) ? kP32W : bw_path_primes(path);
+}
+static const uint64_t* plan_gens(int path, bool w64) {
+    return (w64 && path == BW_PATH_P32) ? kG32W : path == BW_PATH_P64 ? kG64 : kG32;
+}
 
 // ------------------------------------------------------------------ plan
 
@@ -164,7 +180,11 @@ struct TableBuilder {
     }
 };
 
-inline void set_c(Ar32&, uint64_t) {}
+inline void set_c(Ar32& a, uint64_t p) {
+    a.r32 = (uint32_t)(((uint64_t)1 << 32) % p);
+    a.r32q = (uint32_t)shoup_pre(a.r32, p, 32);
+    a.oneq = (uint32_t)(((uint64_t)1 << 32) / p);
+}
 inline void set_c(Ar64& a, uint64_t p) {
     a.c = (uint32_t)(p >> 32);
     a.c3 = 3u * a.c;
@@ -180,15 +200,15 @@ template <class Ar>
 int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     using T = typename Ar::T;
     const int bits = Ar::BITS;
-    const uint64_t* P = pl->path == BW_PATH_P64 ? kP64 : kP32;
-    const uint64_t* Gn = pl->path == BW_PATH_P64 ? kG64 : kG32;
+    const uint64_t* P = plan_primes(pl->path, pl->w64 != 0);
+    const uint64_t* Gn = plan_gens(pl->path, pl->w64 != 0);
     TableBuilder<Ar> tb;
     size_t off[kMaxPrimes][12];
     const size_t n = (size_t)1 << pl->log_n;
     // row-level twiddle length: R * C (two passes) or R2 * C (three passes)
     const int log_rr = pl->log_r2 ? pl->log_r2 : pl->log_r;
     const size_t n_row = (size_t)1 << (log_rr + pl->log_c);
-    uint64_t scale_k[kMaxPrimes] = {0, 0, 0};
+    uint64_t scale_k[kMaxPrimes] = {};
     for (int k = 0; k < pl->K; ++k) {
         const uint64_t p = P[k];
         scale_k[k] = mulmod(invmod(n % p, p), powmod(2, bits, p), p);
@@ -271,6 +291,13 @@ int build_tables(bw_plan* pl, PlanDev<Ar>& pd) {
     g.inv2q = (T)shoup_pre(g.inv2, p2, bits);
     g.p01_lo = (uint64_t)((u128)p0 * p1);
     g.p01_hi = (uint64_t)(((u128)p0 * p1) >> 64);
+    if (pl->K == 6) {
+        for (int i = 1; i < 6; ++i)
+            for (int j = 0; j < i; ++j) {
+                const uint64_t v = invmod(P[j] % P[i], P[i]);
+                g.inv6[i * (i - 1) / 2 + j] = Tw<T>{(T)v, (T)shoup_pre(v, P[i], bits)};
+            }
+    }
     pd.K = pl->K;
     pd.log_n = pl->log_n;
     pd.log_r = pl->log_r;
@@ -326,16 +353,23 @@ int bw_check_size(int path, int K, size_t la, size_t lb, int* log_n_out) {
 // coefficients per operand; every coefficient of the product is below
 // min(na, nb) 2^128, far under p0 p1 p2 (2^184.9) for any size the
 // transform reaches, and all three primes carry it (none is redundant).
-int bw_check_size_w64(size_t la, size_t lb, int* log_n_out) {
+// On the 32-bit path (six primes, v2(p - 1) >= 23) the transform reaches 2^23
+// points, 2^23-word operands; the six primes' product (2^177) bounds every
+// coefficient there (min(na, nb) 2^128 <= 2^150).
+int bw_check_size_w64(size_t la, size_t lb, int* log_n_out, int path = BW_PATH_P64) {
     if (la == 0 || lb == 0) return bw_fail(BW_ESIZE, "operand limb count must be positive");
     const size_t nca = (la + 1) / 2, ncb = (lb + 1) / 2;
     const int log_n = std::max(4, ceil_log2(nca + ncb - 1));
-    const int max_log = bw_path_max_log_n(BW_PATH_P64, 3);
+    int max_log = bw_path_max_log_n(BW_PATH_P64, 3);
+    if (path == BW_PATH_P32) {
+        max_log = 64;
+        for (int k = 0; k < 6; ++k) max_log = std::min(max_log, v2(kP32W[k] - 1));
+    }
     if (log_n > max_log)
         return bw_fail(BW_ESIZE,
-                       "transform length 2^%d for %zu x %zu words exceeds the 64-bit path limit "
-                       "2^%d",
-                       log_n, la, lb, max_log);
+                       "transform length 2^%d for %zu x %zu words exceeds the %d-bit path limit "
+                       "for 64-bit coefficients 2^%d",
+                       log_n, la, lb, path == BW_PATH_P32 ? 32 : 64, max_log);
     if (log_n_out) *log_n_out = log_n;
     return BW_OK;
 }
@@ -388,21 +422,35 @@ int bw_choose_path(int K, size_t la, size_t lb, bool w64_ok) {
 static int resolve_plan(int path, int num_primes, size_t la, size_t lb, unsigned flags,
                         int* path_out, int* K_out, bool* w64_out) {
     int K = num_primes == 0 ? 2 : num_primes;
-    const bool force64 = (flags & BW_PLAN_COEF64) != 0;
-    if (path == BW_PATH_AUTO)
+    bool force64 = (flags & BW_PLAN_COEF64) != 0;
+    if (path == BW_PATH_AUTO) {
         path = force64 ? BW_PATH_P64
                        : bw_choose_path(K < 2 || K > 3 ? 2 : K, la, lb, num_primes == 0);
+        // a single product the 16-bit split leaves: 64-bit coefficients on
+        // the 32-bit path (six primes) while their transform fits (n <= 2^23);
+        // on a B200 they measured faster than the 64-bit path's from 2^20-word
+        // operands (0.206 vs 0.213 ms; 2^21 words 0.347 vs 0.387, 2^22 0.690
+        // vs 0.760, 2^23 1.356 vs 1.514 ms)
+        if (!force64 && num_primes == 0 && path == BW_PATH_P64) {
+            if (bw_check_size_w64(la, lb, nullptr, BW_PATH_P32) == BW_OK) {
+                path = BW_PATH_P32;
+                force64 = true;
+            } else {
+                bw_clear_error();
+            }
+        }
+    }
     bool w64 = false;
     if (force64) {
-        if (path != BW_PATH_P64)
-            return bw_fail(BW_EINVAL, "64-bit coefficients need the 64-bit path");
-        if (num_primes != 0 && num_primes != 3)
-            return bw_fail(BW_EINVAL, "64-bit coefficients need num_primes 3 (or 0)");
+        const int kw = path == BW_PATH_P32 ? 6 : 3;
+        if (num_primes != 0 && num_primes != kw)
+            return bw_fail(BW_EINVAL, "64-bit coefficients need num_primes %d (or 0) on the "
+                                      "%d-bit path", kw, path == BW_PATH_P32 ? 32 : 64);
         w64 = true;
     } else if (num_primes == 0 && path == BW_PATH_P64) {
         w64 = bw_w64_pays(la, lb);
     }
-    if (w64) K = 3;
+    if (w64) K = path == BW_PATH_P32 ? 6 : 3;
     *path_out = path;
     *K_out = K;
     *w64_out = w64;
@@ -498,7 +546,26 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         // the residues count there.
         pl->tw_smem_r =
             ((flags & BW_PLAN_TW_SMEM) && ((size_t)2 * w << pl->log_r) <= 32768) ? 1 : 0;
-        const size_t cbytes = path == BW_PATH_P32 ? 2 : mode == 2 ? 0 : pl->w64 ? 8 : 4;
+        // 64-bit coefficients on the 32-bit path: the forward column pass
+        // loops over the six primes with a u64 copy of the coefficients beside
+        // the residue tile, or (BW_PLAN_K1_ONE_PRIME) runs one prime per CTA
+        // and reduces the coefficients straight into its tile; the loop
+        // measured 0.3-4% faster from 2^20- to 2^23-word operands
+        pl->k1_pp = (path == BW_PATH_P32 && pl->w64 && mode == 2 &&
+                     (flags & BW_PLAN_K1_ONE_PRIME))
+                        ? 1
+                        : 0;
+        // operands that both fill at most half the rows (the zero pad): only
+        // those rows' coefficients are staged, so the u64 copy takes half
+        pl->coef_half = (path == BW_PATH_P32 && pl->w64 && mode == 2 && !pl->k1_pp &&
+                         pl->zt_a && pl->zt_b)
+                            ? 1
+                            : 0;
+        const size_t cbytes = path == BW_PATH_P32
+                                  ? (pl->w64 ? (pl->k1_pp ? 0 : pl->coef_half ? 4 : 8) : 2)
+                              : mode == 2         ? 0
+                              : pl->w64           ? 8
+                                                  : 4;
         const size_t tsb = pl->tw_smem_r ? ((size_t)2 * w << pl->log_r) : 0;
         auto fits1 = [&](int cb) {
             const size_t elems = (size_t)1 << (pl->log_r + cb);
@@ -546,7 +613,7 @@ int bw_plan_setup(bw_plan* pl, int path, int K, int log_n, unsigned flags, int m
         pl->lo = ((pl->log_r2 ? pl->log_r2 : pl->log_r) + pl->log_c + 1) / 2;
         pl->lo_out = (log_n + 1) / 2;
     }
-    for (int k = 0; k < K; ++k) pl->primes[k] = bw_path_primes(path)[k];
+    for (int k = 0; k < K; ++k) pl->primes[k] = plan_primes(path, pl->w64 != 0)[k];
     cudaGetDevice(&pl->device);
     const int rc =
         path == BW_PATH_P64 ? build_tables<Ar64>(pl, pl->pd64) : build_tables<Ar32>(pl, pl->pd32);
@@ -567,7 +634,7 @@ extern "C" int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb, int
     int rc = resolve_plan(path, num_primes, la, lb, flags, &path, &K, &w64);
     if (rc) return rc;
     int log_n = 0;
-    rc = w64 ? bw_check_size_w64(la, lb, &log_n) : bw_check_size(path, K, la, lb, &log_n);
+    rc = w64 ? bw_check_size_w64(la, lb, &log_n, path) : bw_check_size(path, K, la, lb, &log_n);
     if (rc) return rc;
     bw_plan* pl = new bw_plan();
     pl->la = la;
@@ -601,7 +668,7 @@ extern "C" int bw_plan_destroy(bw_plan* pl) {
 // 2n (64-bit coefficients).
 static size_t coef_words(const bw_plan* pl) {
     const size_t n = (size_t)1 << pl->log_n;
-    return pl->path == BW_PATH_P32 ? n / 2 : pl->w64 ? 2 * n : n;
+    return pl->w64 ? 2 * n : pl->path == BW_PATH_P32 ? n / 2 : n;
 }
 
 static size_t ctx_bytes(const bw_plan* pl) {
@@ -620,13 +687,13 @@ extern "C" int bw_plan_get_info(const bw_plan* pl, bw_plan_info* o) {
     o->log_n = pl->log_n;
     o->log_rows = pl->log_r;
     o->log_cols = pl->log_c;
-    o->coeff_bits = pl->path == BW_PATH_P32 ? 16 : pl->w64 ? 64 : 32;
+    o->coeff_bits = pl->w64 ? 64 : pl->path == BW_PATH_P32 ? 16 : 32;
     o->la = pl->la;
     o->lb = pl->lb;
     o->lc = pl->la + pl->lb;
     o->plan_device_bytes = pl->table_bytes;
     o->ctx_device_bytes = ctx_bytes(pl);
-    for (int k = 0; k < 3; ++k) o->primes[k] = k < pl->K ? pl->primes[k] : 0;
+    for (int k = 0; k < kMaxPrimes; ++k) o->primes[k] = k < pl->K ? pl->primes[k] : 0;
     return BW_OK;
 }
 
@@ -901,6 +968,13 @@ int set_smem_attrs() {
         set((const void*)k_row<Ar, 256, 3>);
         set((const void*)k_row<Ar, 512, 3>);
         if constexpr (sizeof(typename Ar::T) == 4) set((const void*)k_row<Ar, 256, 4, true>);
+        if constexpr (sizeof(typename Ar::T) == 4 && !SPLIT16) {
+            // 64-bit coefficients on the 32-bit path
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true, false>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, true, false>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, true, true, true>);
+            set((const void*)k_fwd_col<Ar, SPLIT16, 4, false, true, true>);
+        }
         set((const void*)k_mid_col<Ar, false>);
         set((const void*)k_mid_col<Ar, true>);
         set((const void*)k_inv_col_tma<Ar, 4>);
@@ -1035,7 +1109,7 @@ int copy_chunks_for(const bw_ctx* c, bool ordered) {
     want = std::min(std::min(want, tiles1), kMaxCopyChunks);
     int S = 1;
     while (S * 2 <= want) S *= 2;
-    const int cpw = pl->path == BW_PATH_P32 ? 2 : 1;
+    const int cpw = (pl->path == BW_PATH_P32 && !pl->w64) ? 2 : 1;
     if (S > 1 && ((tiles1 / S) << pl->log_cb1) % cpw) S = 1;
     return S;
 }
@@ -1059,17 +1133,38 @@ int enqueue_transform(bw_ctx* c, const uint32_t* a, const uint32_t* b, bool squa
 
     const int CB1 = 1 << pl->log_cb1;
     // the 64-bit path stages the coefficients inside the residue tile and
-    // runs one prime per CTA (grid.y); the 32-bit path keeps a u16 copy
+    // runs one prime per CTA (grid.x = tile * K + prime); so does the 32-bit
+    // path with 64-bit coefficients when asked (BW_PLAN_K1_ONE_PRIME); the
+    // 32-bit path keeps a u16 (16-bit) or u64 (64-bit coefficients) copy
     constexpr bool PP = sizeof(T) == 8;
+    const bool pp32 = W64 && sizeof(T) == 4 && pl->k1_pp;
+    // (64-bit coefficients on the 32-bit path: the u64 copy holds the loaded
+    // rows only, half the tile when both operands fill at most half of it)
+    const size_t coef_rows = (W64 && sizeof(T) == 4 && pl->coef_half) ? (size_t)R / 2 : R;
     const size_t smem1 = tw_bytes + tile_elems((size_t)R * CB1) * sizeof(T) +
-                         (size_t)R * CB1 * (PP ? 0 : SPLIT16 ? 2 : W64 ? 8 : 4);
+                         coef_rows * CB1 * ((PP || pp32) ? 0 : SPLIT16 ? 2 : W64 ? 8 : 4) +
+                         (W64 && sizeof(T) == 4 && !pp32 ? 16 : 0);
     // K1 takes coefficient counts, or word counts for 64-bit coefficients
     const size_t in_a = W64 ? pl->la : pl->nca, in_b = W64 ? pl->lb : pl->ncb;
     const int cols_outer = 1 << (pl->log_c + pl->log_r2);
     const int tiles1 = cols_outer / CB1;
     const unsigned zt = (pl->zt_a ? 1u : 0u) | (pl->zt_b ? 2u : 0u);
     auto k1 = [&](int tile0, int ntiles) {
-        dim3 g1(ntiles * (PP ? pl->K : 1), 1, square ? 1 : 2);
+        dim3 g1(ntiles * ((PP || pp32) ? pl->K : 1), 1, square ? 1 : 2);
+        if constexpr (W64 && sizeof(T) == 4) {
+            if (pp32) {
+                if (ts) {
+                    k_fwd_col<Ar, SPLIT16, 4, true, true, true>
+                        <<<g1, kColThreads, smem1, c->stream>>>(pd, a, in_a, b, in_b, ra, rb, zt,
+                                                                tile0);
+                } else {
+                    k_fwd_col<Ar, SPLIT16, 4, false, true, true>
+                        <<<g1, kColThreads, smem1, c->stream>>>(pd, a, in_a, b, in_b, ra, rb, zt,
+                                                                tile0);
+                }
+                return;
+            }
+        }
         if constexpr (PP) {
             if (pl->rlog_col == 3) {
                 if (ts) {
@@ -1232,7 +1327,10 @@ int enqueue_product(bw_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t* o
     const bw_plan* pl = c->plan;
     const int pieces = io ? io->chunks : 1;
     int rc;
-    if (pl->w64) {
+    if (pl->w64 && pl->path == BW_PATH_P32) {
+        rc = enqueue_transform<Ar32, false, true>(c, a, b, square, timing, io);
+        if (!rc) rc = enqueue_carry<Ar32, false, true>(c, out, pieces);
+    } else if (pl->w64) {
         rc = enqueue_transform<Ar64, false, true>(c, a, b, square, timing, io);
         if (!rc) rc = enqueue_carry<Ar64, false, true>(c, out, pieces);
     } else if (pl->path == BW_PATH_P64) {
@@ -1501,7 +1599,8 @@ extern "C" int bw_size_supported(int path, int num_primes, size_t la, size_t lb)
     bool w64 = false;
     const int rc = resolve_plan(path, num_primes, la, lb, 0, &path, &K, &w64);
     if (rc) return rc;
-    return w64 ? bw_check_size_w64(la, lb, nullptr) : bw_check_size(path, K, la, lb, nullptr);
+    return w64 ? bw_check_size_w64(la, lb, nullptr, path)
+               : bw_check_size(path, K, la, lb, nullptr);
 }
 
 // Plans and contexts of recent one-shot sizes.  The reference builds and

@@ -31,16 +31,19 @@ struct bw_plan {
     int log_r2 = 0;      // three-pass schedule: middle column length (0: two passes)
     int log_cb2 = 0, lo_out = 0;
     int small = 0;       // single-pass plan: the whole n-point transform in one CTA
-    int w64 = 0;         // 64-bit path with 64-bit coefficients (two words each, K = 3)
+    int w64 = 0;         // 64-bit coefficients (two words each): K = 3 on the 64-bit
+                         // path, K = 6 on the 32-bit path
     int tma_cols = 0;    // inverse column tiles by tensor copies (BW_PLAN_TMA_COLS)
     int shfl_rows = 0;   // row pass exchange through warp shuffles (BW_PLAN_SHFL_ROWS)
+    int k1_pp = 0;       // 32-bit path, 64-bit coefficients: one prime per forward-pass CTA
+    int coef_half = 0;   // ... prime loop: both operands in the low half, half the u64 copy
     int device = 0;
     bool zt_a = false, zt_b = false;
     void* d_tables = nullptr;
     size_t table_bytes = 0;
     bw::PlanDev<bw::Ar32> pd32{};
     bw::PlanDev<bw::Ar64> pd64{};
-    uint64_t primes[3] = {0, 0, 0};
+    uint64_t primes[bw::kMaxPrimes] = {};
     bw_stage_order* order = nullptr;  // plans of bw_plan_create only
 };
 

@@ -42,7 +42,10 @@
 
 namespace bw {
 
-constexpr int kMaxPrimes = 3;
+// Primes of a plan: 2 or 3, or 6 on the 32-bit path with 64-bit coefficients.
+constexpr int kMaxPrimes = 6;
+// Primes the digit-sum Garner (16- and 32-bit coefficients) reads.
+constexpr int kDigitPrimes = 3;
 constexpr int kCarryThreads = 256;
 constexpr int kCarryWordsPerThread = 8;
 constexpr int kCarryTileWords = kCarryThreads * kCarryWordsPerThread;  // 2048
@@ -79,6 +82,9 @@ struct GarnerDev {
     T inv2, inv2q;      // (p0 p1)^-1 mod p2
     uint64_t p0;        // p0 as an integer
     uint64_t p01_lo, p01_hi;  // p0 p1 as a 128-bit integer (64-bit coefficients)
+    // six primes (32-bit path, 64-bit coefficients): p_j^-1 mod p_i with
+    // Shoup companions, pair (i, j < i) at index i (i - 1) / 2 + j
+    Tw<T> inv6[15];
 };
 
 template <class Ar>
@@ -370,7 +376,8 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                                              const uint32_t* __restrict__ limbs, size_t ncoef,
                                              typename Ar::T* res, bool zt_in, int tile,
                                              unsigned char* smem_raw, int kp0 = 0) {
-    static_assert(!PP || (sizeof(typename Ar::T) == 8 && !SPLIT16), "PP: 64-bit path");
+    static_assert(!PP || (!SPLIT16 && (sizeof(typename Ar::T) == 8 || W64)),
+                  "PP: 64-bit path, or 64-bit coefficients on the 32-bit path");
     using T = typename Ar::T;
     const bool zt = zt_in && P.log_r > 0;
     const int log_r = P.log_r, log_c = P.log_c + P.log_r2, log_cb = P.log_cb1;
@@ -386,7 +393,11 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
 
     Tw<T>* tws = reinterpret_cast<Tw<T>*>(smem_raw);         // R entries if TS
     T* buf = reinterpret_cast<T*>(smem_raw + (TS ? (size_t)R * sizeof(Tw<T>) : 0));
-    CT* coef = reinterpret_cast<CT*>(buf + tile_elems((size_t)R << log_cb));
+    // 64-bit coefficients after a 4-byte residue tile start at the next 16-byte
+    // boundary (the tile's 17 (R CB / 16) elements may leave it 4 bytes off)
+    size_t coef_off = tile_elems((size_t)R << log_cb) * sizeof(T);
+    if constexpr (W64 && sizeof(T) == 4) coef_off = (coef_off + 15) & ~(size_t)15;
+    CT* coef = reinterpret_cast<CT*>(reinterpret_cast<unsigned char*>(buf) + coef_off);
 
     if constexpr (SPLIT16) {
         if (CB >= 2) {
@@ -412,6 +423,24 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                 coef[e] = (CT)(ci < ncoef ? (__ldg(limbs + (ci >> 1)) >> ((ci & 1) * 16)) & 0xFFFFu
                                           : 0u);
             }
+        }
+    } else if constexpr (W64 && PP && sizeof(T) == 4) {
+        // 32-bit path, one prime per CTA: each 64-bit coefficient is reduced
+        // for this prime on its way into the residue tile (the K CTAs of a
+        // tile run side by side, so the operand words come from L2 after the
+        // first of them)
+        const Ar ar0 = P.pr[kp0].ar;
+        const bool al8 = (reinterpret_cast<uintptr_t>(limbs) & 7u) == 0;
+        for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
+            const size_t wi = 2 * ((size_t)(e >> log_cb) * C + c0 + (e & (CB - 1)));
+            uint64_t x = 0;
+            if (wi + 1 < ncoef) {
+                x = al8 ? __ldg(reinterpret_cast<const unsigned long long*>(limbs + wi))
+                        : ((uint64_t)__ldg(limbs + wi + 1) << 32) | __ldg(limbs + wi);
+            } else if (wi < ncoef) {
+                x = __ldg(limbs + wi);
+            }
+            buf[LayCol<T>::p(e)] = ar0.reduce64(x);
         }
     } else if (W64 && PP && (reinterpret_cast<uintptr_t>(limbs) & 7u) == 0) {
         // 64-bit coefficients of an 8-byte-aligned operand: one 8-byte copy
@@ -491,13 +520,23 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             auto ld = [&](int v, int idx, int p) -> T {
                 if (first) {
                     if (zt && idx >= R / 2) return T(0);
-                    T x = PP ? buf[p] : (T)coef[(idx << log_cb) + v];
-                    if constexpr (W64) {
-                        // a 64-bit coefficient (up to 64p) enters reduced to
-                        // [0, 2p), leaving the transform its headroom
-                        x = ar.reduce_in(x);
+                    if constexpr (W64 && sizeof(T) == 4) {
+                        // 32-bit path: the staged 64-bit coefficient reduced
+                        // to [0, 2p) for this prime (PP: reduced when staged)
+                        if constexpr (PP) {
+                            return buf[p];
+                        } else {
+                            return ar.reduce64(coef[(idx << log_cb) + v]);
+                        }
+                    } else {
+                        T x = PP ? buf[p] : (T)coef[(idx << log_cb) + v];
+                        if constexpr (W64) {
+                            // a 64-bit coefficient (up to 64p) enters reduced
+                            // to [0, 2p), leaving the transform its headroom
+                            x = ar.reduce_in(x);
+                        }
+                        return x;
                     }
-                    return x;
                 }
                 return buf[p];
             };
@@ -1086,15 +1125,15 @@ __device__ __forceinline__ void garner_digits_at(const PlanDev<Ar>& P,
     {
         const Ar a1 = P.pr[1].ar;
         const GarnerDev<Ar>& G = P.gar;
-        T r[kMaxPrimes][E * CPW];
+        T r[kDigitPrimes][E * CPW];
 #pragma unroll
-        for (int kp = 0; kp < kMaxPrimes; ++kp)
+        for (int kp = 0; kp < kDigitPrimes; ++kp)
 #pragma unroll
             for (int q = 0; q < E * CPW; ++q) r[kp][q] = 0;
         if (valid) {
             // 128-bit vector loads of E*CPW consecutive residues per prime
 #pragma unroll
-            for (int kp = 0; kp < kMaxPrimes; ++kp) {
+            for (int kp = 0; kp < kDigitPrimes; ++kp) {
                 if (kp >= P.K) break;
                 const uint4* src = reinterpret_cast<const uint4*>(base + (size_t)kp * pstride);
 #pragma unroll
@@ -1164,12 +1203,12 @@ __device__ __forceinline__ void garner_digits(const PlanDev<Ar>& P,
 // min(na, nb) 2^128 < 2^160, so c2 >= 2^32 flags an error).  The words are
 // the low 32 E bits of V = sum_q c_q 2^(64 q), X = V >> 32 E (< 2^96).
 // Coefficients at or beyond NL / 2 read nothing and are zero.
-template <class Ar, int E, bool NC = true>
-__device__ __forceinline__ void garner_words_w64_at(const PlanDev<Ar>& P,
-                                                    const typename Ar::T* __restrict__ base,
-                                                    size_t pstride, bool valid,
-                                                    uint32_t (&l)[E], uint32_t (&X)[3],
-                                                    uint32_t* bad_out) {
+template <class Ar, int E, bool NC>
+__device__ __forceinline__ void garner3_words_at(const PlanDev<Ar>& P,
+                                                 const typename Ar::T* __restrict__ base,
+                                                 size_t pstride, bool valid,
+                                                 uint32_t (&l)[E], uint32_t (&X)[3],
+                                                 uint32_t* bad_out) {
     using T = typename Ar::T;
     static_assert(sizeof(T) == 8 && E % 4 == 0, "64-bit residues, whole 16-byte loads");
     constexpr int Q = E / 2;
@@ -1224,6 +1263,102 @@ __device__ __forceinline__ void garner_words_w64_at(const PlanDev<Ar>& P,
     X[2] = (uint32_t)acc1;
     bad |= (uint32_t)((acc1 >> 32) != 0);
     *bad_out |= bad;
+}
+
+// Six primes below 2^30 (32-bit path, 64-bit coefficients): the same words
+// and carry-out as garner3_words_at.  The primes ascend, so a digit k_j
+// (< p_j) is already below every later prime.  Mixed radix: k_0 = r_0 and
+// k_i = (...((r_i - k_0) p_0^-1 - k_1) p_1^-1 ... - k_(i-1)) p_(i-1)^-1 mod p_i;
+// c = k_0 + p_0 (k_1 + p_1 (k_2 + p_2 (k_3 + p_3 (k_4 + p_4 k_5)))) < P < 2^178.
+// A product's coefficients stay below min(na, nb) 2^128 <= 2^150, so a top
+// word c2 >= 2^32 flags an error (residues that disagree give a c spread over
+// [0, P)).
+template <class Ar, int E, bool NC>
+__device__ __forceinline__ void garner6_words_at(const PlanDev<Ar>& P,
+                                                 const uint32_t* __restrict__ base,
+                                                 size_t pstride, bool valid, uint32_t (&l)[E],
+                                                 uint32_t (&X)[3], uint32_t* bad_out) {
+    constexpr int Q = E / 2;
+    static_assert(Q % 4 == 0, "whole 16-byte loads");
+    uint32_t r[6][Q];
+#pragma unroll
+    for (int kp = 0; kp < 6; ++kp)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) r[kp][q] = 0;
+    if (valid) {
+#pragma unroll
+        for (int kp = 0; kp < 6; ++kp) {
+            const uint4* src = reinterpret_cast<const uint4*>(base + (size_t)kp * pstride);
+#pragma unroll
+            for (int h = 0; h < Q / 4; ++h) {
+                const uint4 v = NC ? __ldg(src + h) : src[h];
+                r[kp][4 * h] = v.x;
+                r[kp][4 * h + 1] = v.y;
+                r[kp][4 * h + 2] = v.z;
+                r[kp][4 * h + 3] = v.w;
+            }
+        }
+    }
+    const GarnerDev<Ar>& G = P.gar;
+    uint32_t bad = 0;
+    uint64_t acc0 = 0, acc1 = 0;  // running carry (< 2^96)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        uint32_t k[6];
+        k[0] = r[0][q];
+#pragma unroll
+        for (int i = 1; i < 6; ++i) {
+            const Ar ai = P.pr[i].ar;
+            uint32_t t = r[i][q];
+#pragma unroll
+            for (int j = 0; j < i; ++j) {
+                const uint32_t d = t - k[j];  // t, k_j < p_i
+                t = min(d, d + ai.p);
+                const Tw<uint32_t> iv = G.inv6[i * (i - 1) / 2 + j];
+                t = ai.red1(ai.shoup(t, iv.w, iv.wq));
+            }
+            k[i] = t;
+        }
+        const uint64_t v4 = (uint64_t)k[5] * P.pr[4].ar.p + k[4];                  // < 2^60
+        const unsigned __int128 v3 = (unsigned __int128)v4 * P.pr[3].ar.p + k[3];  // < 2^90
+        const unsigned __int128 v2 = v3 * P.pr[2].ar.p + k[2];                     // < 2^120
+        // v2 p1 + k1 (< 2^150), then times p0 plus k0, in 64-bit words
+        const unsigned __int128 a0 = (unsigned __int128)(uint64_t)v2 * P.pr[1].ar.p + k[1];
+        const unsigned __int128 a1 =
+            (unsigned __int128)(uint64_t)(v2 >> 64) * P.pr[1].ar.p + (uint64_t)(a0 >> 64);
+        const uint64_t p0 = P.pr[0].ar.p;
+        const unsigned __int128 m0 = (unsigned __int128)(uint64_t)a0 * p0 + k[0];
+        const unsigned __int128 m1 = (unsigned __int128)(uint64_t)a1 * p0 + (uint64_t)(m0 >> 64);
+        const uint64_t c0 = (uint64_t)m0, c1 = (uint64_t)m1;
+        const uint64_t c2 = (uint64_t)(a1 >> 64) * p0 + (uint64_t)(m1 >> 64);
+        bad |= (uint32_t)((c2 >> 32) != 0);
+        const unsigned __int128 s0 = (unsigned __int128)acc0 + c0;
+        l[2 * q] = (uint32_t)s0;
+        l[2 * q + 1] = (uint32_t)((uint64_t)s0 >> 32);
+        const unsigned __int128 s1 = (unsigned __int128)acc1 + c1 + (uint64_t)(s0 >> 64);
+        acc0 = (uint64_t)s1;
+        acc1 = c2 + (uint64_t)(s1 >> 64);
+    }
+    X[0] = (uint32_t)acc0;
+    X[1] = (uint32_t)(acc0 >> 32);
+    X[2] = (uint32_t)acc1;
+    bad |= (uint32_t)((acc1 >> 32) != 0);
+    *bad_out |= bad;
+}
+
+// 64-bit coefficients: three 58-bit primes (64-bit path) or six 30-bit
+// primes (32-bit path).
+template <class Ar, int E, bool NC = true>
+__device__ __forceinline__ void garner_words_w64_at(const PlanDev<Ar>& P,
+                                                    const typename Ar::T* __restrict__ base,
+                                                    size_t pstride, bool valid,
+                                                    uint32_t (&l)[E], uint32_t (&X)[3],
+                                                    uint32_t* bad_out) {
+    if constexpr (sizeof(typename Ar::T) == 4) {
+        garner6_words_at<Ar, E, NC>(P, base, pstride, valid, l, X, bad_out);
+    } else {
+        garner3_words_at<Ar, E, NC>(P, base, pstride, valid, l, X, bad_out);
+    }
 }
 
 template <class Ar, int E, bool NC = true>

@@ -13,7 +13,7 @@ benchmarks are quoted on:
 """
 import numpy as np
 
-from ._lib import BW_PATH_P32, BW_PATH_P64
+from ._lib import BW_PATH_P32, BW_PATH_P64, BW_PLAN_COEF64
 
 
 def rand_operand(rng, words):
@@ -81,18 +81,23 @@ def serving_sizes(count, seed=5, lo_log=10, hi_log=24, square_frac=0.2):
 #   literal           (path, num_primes, flags) of the workload as the
 #                     reference states it (its coefficient width and prime
 #                     count), timed beside the library's choice
+#   other             (optional) the same product on the other prime path,
+#                     timed beside it: the 32-bit path with 64-bit
+#                     coefficients (six primes) for the 2^28-bit workloads
 PLAIN = {
     "2": dict(
         words_a=1 << 23, words_b=1 << 23, seeds=(1234, 5678), square=False,
         plan=(BW_PATH_P64, 0, 0),
         expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=23, log_cols=12),
         ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
+        other=(BW_PATH_P32, 0, BW_PLAN_COEF64),
         desc="plain 2^28-bit x 2^28-bit product"),
     "2sq": dict(
         words_a=1 << 23, words_b=1 << 23, seeds=(1234, 1234), square=True,
         plan=(BW_PATH_P64, 0, 0),
         expect=dict(path=64, coeff_bits=64, num_primes=3, log_n=23, log_cols=12),
         ref=(64, 2), literal=(BW_PATH_P64, 2, 0),
+        other=(BW_PATH_P32, 0, BW_PLAN_COEF64),
         desc="squaring of a 2^28-bit integer"),
     "1": dict(
         words_a=1 << 15, words_b=1 << 15, seeds=(1234, 5678), square=False,
@@ -131,6 +136,10 @@ def plain_plan_args(name, which="plan"):
     w = PLAIN[name]
     path, k, flags = w[which]
     return w["words_a"], w["words_b"], path, k, flags
+
+
+# what the `other` plans resolve to (bw_plan_info fields)
+OTHER_EXPECT = dict(path=32, coeff_bits=64, num_primes=6)
 
 
 def algorithm_of(info):

@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define BW_ABI_VERSION 1
+#define BW_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define BW_OK            0
@@ -84,12 +84,15 @@ extern "C" {
 /* Column-pass tiles of up to 128 KiB of residues instead of 64 KiB (twice
  * the columns per CTA: longer contiguous row segments, fewer CTAs per SM). */
 #define BW_PLAN_WIDE_COLS   (1u << 19)
-/* 64-bit path with 64-bit coefficients (two words each) and three primes,
- * all three carrying the coefficients (no redundant prime): half the
- * transform length of 32-bit coefficients for 1.5x the primes.  num_primes 0
- * on the 64-bit path chooses it where it halves a transform of at least 2^19
- * points; this flag forces it (num_primes must be 0 or 3).  The reference splits operands into
- * 32-bit coefficients only (src/zero_pad.cu:3-57); the product is the same. */
+/* 64-bit coefficients (two words each).  On the 64-bit path: three primes,
+ * all three carrying the coefficients (no redundant prime), half the
+ * transform length of 32-bit coefficients for 1.5x the primes; num_primes 0
+ * there chooses it where it halves a transform of at least 2^19 points.  On
+ * the 32-bit path: six primes below 2^30 (transforms of up to 2^23 points,
+ * operands up to 2^23 words), a quarter of the 16-bit coefficients' transform
+ * length for 3x the primes.  With this flag num_primes must be 0, or 3 (64-bit
+ * path) or 6 (32-bit path).  The reference splits operands into 32-bit
+ * coefficients only (src/zero_pad.cu:3-57); the product is the same. */
 #define BW_PLAN_COEF64      (1u << 20)
 /* Radix-16 rounds in the row pass where radix 8 is the default (single
  * products on the 64-bit path with rows of at most 2^12 points). */
@@ -109,6 +112,11 @@ extern "C" {
  * inside each half-warp) instead of shared memory.  A measured alternative,
  * off by default. */
 #define BW_PLAN_SHFL_ROWS   (1u << 25)
+/* 32-bit path with 64-bit coefficients: the forward column pass runs one
+ * prime per CTA, reducing the coefficients straight into its residue tile,
+ * instead of looping over the six primes in one CTA with a u64 copy of the
+ * tile's coefficients beside its residues (the default, measured faster). */
+#define BW_PLAN_K1_ONE_PRIME (1u << 26)
 
 /* ---- flags for bw_multiply ------------------------------------------------ */
 #define BW_PTR_HOST    0u    /* a, b, c are host pointers (pinned or pageable):
@@ -163,7 +171,7 @@ typedef struct bw_plan_info {
     size_t   lc;            /* product length in u32 words (= la + lb)       */
     size_t   plan_device_bytes;   /* twiddle + constant tables               */
     size_t   ctx_device_bytes;    /* scratch one context allocates           */
-    uint64_t primes[3];
+    uint64_t primes[6];     /* the first num_primes entries are set          */
 } bw_plan_info;
 
 typedef struct bw_limits_info {
@@ -189,14 +197,15 @@ int bw_size_supported(int path, int num_primes, size_t la, size_t lb);
 
 /* Build the plan (twiddle tables on the device, Garner constants) for
  * products of la x lb u32 words.  num_primes = 0 lets the library choose:
- * with path = BW_PATH_AUTO, the 32-bit path (16-bit coefficients, K = 2)
+ * with path = BW_PATH_AUTO, the 32-bit path with 16-bit coefficients (K = 2)
  * while its transform has at most 2^21 points (operands up to about 2^24
- * bits), the 64-bit path beyond; on the 64-bit path, 64-bit coefficients
- * with K = 3 (BW_PLAN_COEF64) where they halve the transform and it has at
- * least 2^19 points, else 32-bit coefficients with K = 2.  num_primes 2 or
- * 3 keeps the reference's 16- or 32-bit coefficients (and then AUTO takes
- * the 32-bit path up to 2^24 points).  The plan is bound to the current
- * CUDA device. */
+ * bits), then the 32-bit path with 64-bit coefficients (K = 6) while its
+ * transform has at most 2^23 points (operands up to 2^28 bits), the 64-bit
+ * path beyond; on the 64-bit path, 64-bit coefficients with K = 3
+ * (BW_PLAN_COEF64) where they halve the transform and it has at least 2^19
+ * points, else 32-bit coefficients with K = 2.  num_primes 2 or 3 keeps the
+ * reference's 16- or 32-bit coefficients (and then AUTO takes the 32-bit path
+ * up to 2^24 points).  The plan is bound to the current CUDA device. */
 int bw_plan_create(bw_plan** out, int path, size_t la, size_t lb,
                    int num_primes, unsigned flags);
 int bw_plan_destroy(bw_plan* plan);

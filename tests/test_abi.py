@@ -29,7 +29,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version():
-    assert bw.lib.bw_abi_version() == 1
+    assert bw.lib.bw_abi_version() == 2
 
 
 def test_limits():

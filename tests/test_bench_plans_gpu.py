@@ -45,7 +45,8 @@ def plans_of(name):
     """The benchmarked plan and, if different, the workload as the reference
     states it (its coefficient width and prime count)."""
     w = workloads.PLAIN[name]
-    return ["plan"] + (["literal"] if w["literal"] != w["plan"] else [])
+    return (["plan"] + (["literal"] if w["literal"] != w["plan"] else []) +
+            (["other"] if w.get("other") else []))
 
 
 @pytest.mark.parametrize("name,which", [(n, k) for n in ("1", "2", "2sq", "prof", "prof32")
@@ -58,6 +59,9 @@ def test_benchmarked_plan_bit_exact(name, which):
     with bw.Plan(la, lb, path, k, flags=flags) as p, bw.Context(p) as c:
         if which == "plan":
             for key, v in w["expect"].items():
+                assert p.info[key] == v, (key, p.info[key], v)
+        if which == "other":
+            for key, v in workloads.OTHER_EXPECT.items():
                 assert p.info[key] == v, (key, p.info[key], v)
         got = c.square(a) if w["square"] else c.multiply(a, b)
         assert (got == want).all()

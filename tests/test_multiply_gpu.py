@@ -401,13 +401,18 @@ def test_p32_longest_transform_vs_gmp():
 
 
 def test_automatic_path_choice():
-    # num_primes 0: the 32-bit path while its transform has at most 2^21
-    # points, then the 64-bit path with 64-bit coefficients
-    for la, lb, want, bits in [(1, 1, 32, 16), (1000, 700, 32, 16), (1 << 19, 1 << 19, 32, 16),
-                               (1 << 19, (1 << 19) + 1, 64, 64), (1 << 22, 1 << 22, 64, 64),
-                               (1 << 23, 1 << 23, 64, 64)]:
+    # num_primes 0: the 32-bit path with 16-bit coefficients while its
+    # transform has at most 2^21 points, then the 32-bit path with 64-bit
+    # coefficients (six primes) up to 2^23 points, then the 64-bit path with
+    # 64-bit coefficients
+    for la, lb, want, bits, k in [(1, 1, 32, 16, 2), (1000, 700, 32, 16, 2),
+                                  (1 << 19, 1 << 19, 32, 16, 2),
+                                  (1 << 19, (1 << 19) + 1, 32, 64, 6),
+                                  (1 << 22, 1 << 22, 32, 64, 6), (1 << 23, 1 << 23, 32, 64, 6),
+                                  ((1 << 23) + 2, (1 << 23) + 2, 64, 64, 3)]:
         with bw.Plan(la, lb) as p:
-            assert (p.info["path"], p.info["coeff_bits"]) == (want, bits), (la, lb, p.info)
+            got = (p.info["path"], p.info["coeff_bits"], p.info["num_primes"])
+            assert got == (want, bits, k), (la, lb, p.info)
     # the 64-bit path below the 64-bit-coefficient threshold keeps 32-bit ones
     with bw.Plan(1 << 18, 1 << 18, 64) as p:
         assert p.info["coeff_bits"] == 32 and p.info["num_primes"] == 2
@@ -602,8 +607,9 @@ def test_coef64_copies_pointers_and_choice():
     for K in (2, 3):
         with bw.Plan(la, lb, 64, K) as p:
             assert p.info["coeff_bits"] == 32 and p.info["num_primes"] == K
+    # 64-bit coefficients take 3 primes on the 64-bit path, 6 on the 32-bit one
     with pytest.raises(bw.BwError):
-        bw.Plan(100, 100, 32, 0, flags=COEF64)
+        bw.Plan(100, 100, 32, 2, flags=COEF64)
     with pytest.raises(bw.BwError):
         bw.Plan(100, 100, 64, 2, flags=COEF64)
 
