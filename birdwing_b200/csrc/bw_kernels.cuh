@@ -294,12 +294,17 @@ __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
 // whose shared-memory tile slot is p (tile element (idx << log_cb) + v in
 // layout L).  LIN: the round's stride D = d + log_cb lets the slots advance
 // by a fixed stride (L::stride); otherwise each offset is computed (L::off).
-template <class Ar, class L, int RL, bool INV, bool TS, bool LIN, class LD, class ST>
-__device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
+// FCB >= 0: the round has stride 1 in the vector (d_log = 0) and the batch
+// width is 2^FCB, both known at compile time, so that every slot offset is an
+// immediate (a tile's stride-1 round; log_cb is then ignored).
+template <class Ar, class L, int RL, bool INV, bool TS, bool LIN, int FCB = -1, class LD,
+          class ST>
+__device__ __forceinline__ void run_round(int log_len, int log_cb_rt, int s0,
                                           const Tw<typename Ar::T>* __restrict__ W,
                                           const Ar& ar, bool zt, LD ld, ST st) {
     using T = typename Ar::T;
-    const int d_log = log_len - s0 - RL;
+    const int log_cb = FCB >= 0 ? FCB : log_cb_rt;
+    const int d_log = FCB >= 0 ? 0 : log_len - s0 - RL;
     const int D = d_log + log_cb;
     const int S = L::stride(D);
     const int nsub = 1 << (log_cb + log_len - RL);
@@ -327,21 +332,56 @@ __device__ __forceinline__ void run_round(int log_len, int log_cb, int s0,
 
 // Dispatch on the round's radix and addressing: only the remainder round (the
 // first round of a transform) is narrower than 2^RLOG, so the full radix has
-// one instantiation per call site and the narrow ones stay small; a round
-// whose stride the layout cannot step through linearly computes its offsets.
+// one instantiation per call site and the narrow ones stay small.  A round
+// whose stride the layout steps through linearly adds one stride per slot; a
+// stride-1 round of a tile up to 16 vectors wide gets compile-time offsets;
+// the others compute their offsets.
 template <class Ar, class L, int RLOG, bool INV, bool TS, class LD, class ST>
 __device__ __forceinline__ void run_round_rl(int rl, int log_len, int log_cb, int s0,
                                              const Tw<typename Ar::T>* __restrict__ W,
                                              const Ar& ar, bool zt, LD ld, ST st) {
-    const int D = log_len - s0 - rl + log_cb;
+    const int d_log = log_len - s0 - rl;
+    const int D = d_log + log_cb;
     if (rl == RLOG) {
+        // (4-byte residues only: on the 64-bit path the extra instantiations
+        // measured slower, the inverse column pass 0.231 -> 0.247 ms)
+        if constexpr (sizeof(typename Ar::T) == 4) {
+            if (d_log == 0 && log_cb <= 4) {
+                switch (log_cb) {
+                    case 0:
+                        run_round<Ar, L, RLOG, INV, TS, false, 0>(log_len, 0, s0, W, ar,
+                                                                  zt, ld, st);
+                        return;
+                    case 1:
+                        run_round<Ar, L, RLOG, INV, TS, false, 1>(log_len, 1, s0, W, ar,
+                                                                  zt, ld, st);
+                        return;
+                    case 2:
+                        run_round<Ar, L, RLOG, INV, TS, false, 2>(log_len, 2, s0, W, ar,
+                                                                  zt, ld, st);
+                        return;
+                    case 3:
+                        run_round<Ar, L, RLOG, INV, TS, false, 3>(log_len, 3, s0, W, ar,
+                                                                  zt, ld, st);
+                        return;
+                    default:
+                        run_round<Ar, L, RLOG, INV, TS, false, 4>(log_len, 4, s0, W, ar,
+                                                                  zt, ld, st);
+                        return;
+                }
+            }
+        }
         if (L::lin(D)) {
             run_round<Ar, L, RLOG, INV, TS, true>(log_len, log_cb, s0, W, ar, zt, ld, st);
         } else {
             run_round<Ar, L, RLOG, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
         }
     } else if (rl == 3) {
-        run_round<Ar, L, 3, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        if (L::lin(D)) {
+            run_round<Ar, L, 3, INV, TS, true>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        } else {
+            run_round<Ar, L, 3, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
+        }
     } else if (rl == 2) {
         run_round<Ar, L, 2, INV, TS, false>(log_len, log_cb, s0, W, ar, zt, ld, st);
     } else {
@@ -459,6 +499,7 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
             }
         }
     } else {
+        const bool al8 = (reinterpret_cast<uintptr_t>(limbs) & 7u) == 0;
         for (int e = threadIdx.x; e < (rows_loaded << log_cb); e += blockDim.x) {
             const size_t ci = (size_t)(e >> log_cb) * C + c0 + (e & (CB - 1));
             if constexpr (PP) {
@@ -476,18 +517,24 @@ __device__ __forceinline__ void fwd_col_body(const PlanDev<Ar>& P,
                     dst[1] = 0;
                 }
             } else if constexpr (W64) {
-                // two 4-byte copies: the operand may start at an odd word
+                // one 8-byte copy from an 8-byte-aligned operand, else two
+                // 4-byte copies (the operand may start at an odd word)
                 uint32_t* dst = reinterpret_cast<uint32_t*>(coef + e);
                 const size_t wi = 2 * ci;
-                if (wi < ncoef) {
-                    cp_async_elem(dst, limbs + wi);
+                if (al8 && wi + 1 < ncoef) {
+                    cp_async_elem(reinterpret_cast<uint64_t*>(dst),
+                                  reinterpret_cast<const uint64_t*>(limbs + wi));
                 } else {
-                    dst[0] = 0;
-                }
-                if (wi + 1 < ncoef) {
-                    cp_async_elem(dst + 1, limbs + wi + 1);
-                } else {
-                    dst[1] = 0;
+                    if (wi < ncoef) {
+                        cp_async_elem(dst, limbs + wi);
+                    } else {
+                        dst[0] = 0;
+                    }
+                    if (wi + 1 < ncoef) {
+                        cp_async_elem(dst + 1, limbs + wi + 1);
+                    } else {
+                        dst[1] = 0;
+                    }
                 }
             } else {
                 // 32-bit limbs land in shared memory without passing registers
@@ -968,9 +1015,11 @@ __device__ __forceinline__ void inv_col_body(const PlanDev<Ar>& P, typename Ar::
 // (cp.async.bulk.tensor.3d, CB columns x BR rows of prime blockIdx.y, no
 // multicast) that complete on a shared-memory mbarrier; every thread waits on
 // it (bounded).  A tensor copy writes its box densely, so the rounds run on an
-// unpadded tile (its stride-CB first round has bank conflicts the padded
-// layouts avoid); it is the measured alternative to the per-element cp.async
-// of k_inv_col.
+// unpadded tile: its stride-1 round (a thread reads 16 consecutive rows of one
+// column, rows CB words apart) puts the sub-problems of a warp 16 CB words
+// apart, on the same banks.  Padding between boxes cannot spread them: a box
+// must land on a 128-byte boundary, so any pad is whole bank cycles.  The
+// measured alternative to the per-element cp.async of k_inv_col.
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -1309,15 +1358,15 @@ __device__ __forceinline__ void garner6_words_at(const PlanDev<Ar>& P,
 #pragma unroll
         for (int i = 1; i < 6; ++i) {
             const Ar ai = P.pr[i].ar;
+            // t stays in [0, 2p_i): t - k_j + p_i < 3p_i < 2^32 is a valid
+            // Shoup input, and only the digit itself is reduced to [0, p_i)
             uint32_t t = r[i][q];
 #pragma unroll
             for (int j = 0; j < i; ++j) {
-                const uint32_t d = t - k[j];  // t, k_j < p_i
-                t = min(d, d + ai.p);
                 const Tw<uint32_t> iv = G.inv6[i * (i - 1) / 2 + j];
-                t = ai.red1(ai.shoup(t, iv.w, iv.wq));
+                t = ai.shoup(t - k[j] + ai.p, iv.w, iv.wq);  // k_j < p_j < p_i
             }
-            k[i] = t;
+            k[i] = ai.red1(t);
         }
         const uint64_t v4 = (uint64_t)k[5] * P.pr[4].ar.p + k[4];                  // < 2^60
         const unsigned __int128 v3 = (unsigned __int128)v4 * P.pr[3].ar.p + k[3];  // < 2^90

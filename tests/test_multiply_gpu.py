@@ -641,8 +641,10 @@ def test_tma_inverse_columns_exact():
     for la, lb in [(1, 1), (3000, 1777), (65537, 4097), ((1 << 19) + 3, (1 << 18) - 5)]:
         a, b = rand_words(la, rng), rand_words(lb, rng)
         want = gmp_ref.mul(a, b)
-        for path, K in ((64, 0), (64, 2), (32, 2), (32, 3)):
+        for path, K in ((64, 0), (64, 2), (32, 2), (32, 3), (32, 6)):
             for fl in (L.BW_PLAN_TMA_COLS, L.BW_PLAN_NO_TMA_COLS):
+                if K == 6:
+                    fl |= L.BW_PLAN_COEF64
                 with bw.Plan(la, lb, path, K, flags=fl) as p, bw.Context(p) as c:
                     assert (c.multiply(a, b) == want).all(), (la, lb, path, K, fl)
                     if la == lb:

@@ -114,3 +114,24 @@ def test_full_size_device_pointers_exact():
             assert (dc.cpu().numpy().view(np.uint32) == want).all()
         assert (c.multiply(a, b) == want).all()
         assert (c.square(a) == gmp_ref.mul(a, a)).all()
+
+
+def test_odd_word_offsets_exact():
+    # operands at odd word offsets of a device buffer: the forward pass stages
+    # each 64-bit coefficient as two 4-byte copies instead of one 8-byte copy
+    import torch
+    la, lb = 300001, 262147
+    a = mt64.random_words_top_fast(la, 9)
+    b = mt64.random_words_top_fast(lb, 10)
+    want = gmp_ref.mul(a, b)
+    buf = torch.from_numpy(np.concatenate([[7], a, b]).astype(np.uint32).view(np.int32)).cuda()
+    dc = torch.empty(la + lb, dtype=torch.int32, device="cuda")
+    for flags in (0, L.BW_PLAN_K1_ONE_PRIME):
+        with plan(la, lb, flags) as p, bw.Context(p) as c:
+            for _ in range(2):
+                dc.fill_(-1)
+                torch.cuda.synchronize()
+                c.multiply_device(buf.data_ptr() + 4, la, buf.data_ptr() + 4 * (1 + la), lb,
+                                  dc.data_ptr(), la + lb)
+                c.sync()
+                assert (dc.cpu().numpy().view(np.uint32) == want).all(), flags
