@@ -150,7 +150,7 @@ SIGNATURES = {
     "bw_batch_set_wait_limit": (_I, [_P, _I]),
     "bw_batch_inject_wait_fault": (_I, [_P, _I]),
     "bw_tune_table_export": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
-    "bw_tune_table_set": (_I, [_I, _I, _I, _I, _I]),
+    "bw_tune_table_set": (_I, [_I, _I, _I, _I, _I, _I]),
     "bw_server_create": (_I, [ctypes.POINTER(_P), ctypes.POINTER(bw_server_config)]),
     "bw_server_destroy": (_I, [_P]),
     "bw_server_prewarm": (_I, [_P, _I, _I]),

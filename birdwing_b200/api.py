@@ -335,14 +335,19 @@ def tune_table():
     return json.loads(buf.value.decode())
 
 
-def set_tune_entry(path, num_primes, log_n, small, log_cols=0):
-    check(lib.bw_tune_table_set(path, num_primes, log_n, 1 if small else 0, log_cols))
+def set_tune_entry(path, num_primes, log_n, small, log_cols=0, row_radix=0):
+    """One tune-table entry: one CTA per product (small), or the 4-step
+    kernels with 2^log_cols columns (0: automatic) and row rounds of radix
+    row_radix (8 or 16; 0: the path's default)."""
+    check(lib.bw_tune_table_set(path, num_primes, log_n, 1 if small else 0, log_cols,
+                                row_radix))
 
 
 def load_tune_table(entries):
     """Install entries as produced by tune_table() (e.g. read back from JSON)."""
     for e in entries:
-        set_tune_entry(e["path"], e["num_primes"], e["log_n"], e["small"], e["log_cols"])
+        set_tune_entry(e["path"], e["num_primes"], e["log_n"], e["small"], e["log_cols"],
+                       e.get("row_radix", 0))
 
 
 class Server:

@@ -46,7 +46,7 @@ namespace {
                            "%s failed: %s", #call, cudaGetErrorString(e_));               \
     } while (0)
 
-// ---- tune table: (path, K, log_n) -> kernel form and split
+// ---- tune table: (path, K, log_n) -> kernel form, split and row radix
 struct TuneKey {
     int path, K, log_n;
     bool operator<(const TuneKey& o) const {
@@ -56,6 +56,7 @@ struct TuneKey {
 struct TuneVal {
     int small;     // 1: one CTA per product
     int log_cols;  // 4-step split (0 = automatic)
+    int rlog;      // row-pass radix log2, 3 or 4 (0 = the path's default)
     float ms;      // measured time of the bucket when tuned (0 = default)
 };
 std::mutex g_tune_mu;
@@ -78,7 +79,7 @@ TuneVal tune_get(int path, int K, int log_n) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(TuneKey{path, K, log_n});
     if (it != g_tune.end()) return it->second;
-    return TuneVal{log_n <= kSmallDefaultLog ? 1 : 0, 0, 0.f};
+    return TuneVal{log_n <= kSmallDefaultLog ? 1 : 0, 0, 0, 0.f};
 }
 
 struct Prod {
@@ -94,7 +95,7 @@ struct Prod {
 
 struct Bucket {
     int path = 0, K = 2, log_n = 0;
-    int small = 0, log_cols = 0;
+    int small = 0, log_cols = 0, rlog = 0;
     bw_plan plan;
     std::vector<size_t> prods;
     BatchProd* d_desc = nullptr;
@@ -245,10 +246,13 @@ void enqueue_group_t(const bw_group_launch& g, cudaStream_t s) {
     const size_t ntab = 2 * (((size_t)1 << la) + ((size_t)C >> la));
     const size_t smem2 = ntab * sizeof(Tw<T>) + tile_elems(C) * sizeof(T) * 2;
     const dim3 g2(R, pl.K, np);
-    if constexpr (sizeof(T) == 8) {
-        // radix-8 rounds on at most 256 threads (64 registers, as the
-        // single-product row pass of the 64-bit path)
-        switch (std::min(256, std::max(64, C >> 3))) {
+    // row rounds: radix 8 on the 64-bit path (at most 256 threads, 64
+    // registers, as its single-product row pass), radix 16 on the 32-bit
+    // path, unless the tune table chose the other radix for the bucket
+    const int rl = g.rlog ? g.rlog : (sizeof(T) == 8 ? 3 : 4);
+    if (rl == 3) {
+        switch (std::min(sizeof(T) == 8 ? 256 : 512, std::max(64, C >> 3))) {
+            case 512: kb_row<Ar, 512, 3><<<g2, 512, smem2, s>>>(P, g.d_desc, ra, rb); break;
             case 256: kb_row<Ar, 256, 3><<<g2, 256, smem2, s>>>(P, g.d_desc, ra, rb); break;
             case 128: kb_row<Ar, 128, 3><<<g2, 128, smem2, s>>>(P, g.d_desc, ra, rb); break;
             default: kb_row<Ar, 64, 3><<<g2, 64, smem2, s>>>(P, g.d_desc, ra, rb); break;
@@ -289,7 +293,11 @@ int set_group_attrs() {
         set((const void*)kb_inv_col<Ar64, 4>);
         set((const void*)kb_inv_col<Ar32, 4>);
         for (auto f : {(const void*)kb_row<Ar64, 64, 3>, (const void*)kb_row<Ar64, 128, 3>,
-                       (const void*)kb_row<Ar64, 256, 3>,
+                       (const void*)kb_row<Ar64, 256, 3>, (const void*)kb_row<Ar64, 512, 3>,
+                       (const void*)kb_row<Ar64, 64, 4>, (const void*)kb_row<Ar64, 128, 4>,
+                       (const void*)kb_row<Ar64, 256, 4>, (const void*)kb_row<Ar64, 512, 4>,
+                       (const void*)kb_row<Ar32, 64, 3>, (const void*)kb_row<Ar32, 128, 3>,
+                       (const void*)kb_row<Ar32, 256, 3>, (const void*)kb_row<Ar32, 512, 3>,
                        (const void*)kb_row<Ar32, 64, 4>, (const void*)kb_row<Ar32, 128, 4>,
                        (const void*)kb_row<Ar32, 256, 4>, (const void*)kb_row<Ar32, 512, 4>})
             set(f);
@@ -419,6 +427,7 @@ int build_layout(bw_batch* bt) {
             const TuneVal tv = tune_get(p.path, bt->K, p.log_n);
             b.small = tv.small && p.log_n <= small_max_log(p.path);
             b.log_cols = tv.log_cols;
+            b.rlog = tv.rlog;
             index[key] = bt->buckets.size();
             bt->buckets.push_back(std::move(b));
             it = index.find(key);
@@ -542,7 +551,7 @@ int build_layout(bw_batch* bt) {
         if (bt->persistent && bk.small) continue;
         bw_group_launch g{&bk.plan, bk.d_desc, (unsigned)bk.prods.size(), bk.d_res_a,
                           bk.d_res_b, bk.ntiles, bt->d_err, bt->spin_limit,
-                          bt->inject_wait_fault};
+                          bt->inject_wait_fault, bk.rlog};
         rc = bw_enqueue_group(g, bt->side[branch++ % nside]);
     }
     for (int s = 0; s < nside; ++s) {
@@ -793,17 +802,19 @@ extern "C" int bw_batch_autotune(bw_batch* bt, int reps) {
         TuneKey key{p.path, bt->K, p.log_n};
         if (cands.count(key)) continue;
         std::vector<TuneVal> v;
-        if (p.log_n <= small_max_log(p.path)) v.push_back(TuneVal{1, 0, 0.f});
-        // 4-step splits from square to long rows (columns of 2^2 at least)
+        if (p.log_n <= small_max_log(p.path)) v.push_back(TuneVal{1, 0, 0, 0.f});
+        // 4-step splits from square to long rows (columns of 2^2 at least),
+        // each with row rounds of radix 8 and of radix 16
         const int max_c = p.path == BW_PATH_P64 ? 13 : 14;
         for (int lc = (p.log_n + 1) / 2 - 1; lc <= std::min(max_c, p.log_n - 2); ++lc)
-            if (lc >= 2 && p.log_n - lc <= 13) v.push_back(TuneVal{0, lc, 0.f});
+            if (lc >= 2 && p.log_n - lc <= 13)
+                for (int rl = 3; rl <= 4; ++rl) v.push_back(TuneVal{0, lc, rl, 0.f});
         cands[key] = v;
     }
     // one sub-batch per key with the batch's products of that key
     for (auto& kv : cands) {
         const TuneKey key = kv.first;
-        TuneVal best{0, 0, 1e30f};
+        TuneVal best{0, 0, 0, 1e30f};
         for (const TuneVal& cand : kv.second) {
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -842,12 +853,13 @@ extern "C" int bw_tune_table_export(char* buf, size_t len, size_t* needed) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         bool first = true;
         for (const auto& kv : g_tune) {
-            char line[160];
+            char line[200];
             snprintf(line, sizeof line,
                      "%s{\"path\": %d, \"num_primes\": %d, \"log_n\": %d, \"small\": %d, "
-                     "\"log_cols\": %d, \"ms\": %.6f}",
+                     "\"log_cols\": %d, \"row_radix\": %d, \"ms\": %.6f}",
                      first ? "" : ", ", kv.first.path, kv.first.K, kv.first.log_n,
-                     kv.second.small, kv.second.log_cols, kv.second.ms);
+                     kv.second.small, kv.second.log_cols,
+                     kv.second.rlog ? 1 << kv.second.rlog : 0, kv.second.ms);
             s += line;
             first = false;
         }
@@ -862,11 +874,14 @@ extern "C" int bw_tune_table_export(char* buf, size_t len, size_t* needed) {
     return BW_OK;
 }
 
-extern "C" int bw_tune_table_set(int path, int num_primes, int log_n, int small, int log_cols) {
+extern "C" int bw_tune_table_set(int path, int num_primes, int log_n, int small, int log_cols,
+                                 int row_radix) {
     bw_clear_error();
     if (path != BW_PATH_P32 && path != BW_PATH_P64) return bw_fail(BW_EINVAL, "bad path");
+    if (row_radix != 0 && row_radix != 8 && row_radix != 16)
+        return bw_fail(BW_EINVAL, "row_radix must be 0 (the path's default), 8 or 16");
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[TuneKey{path, num_primes == 0 ? 2 : num_primes, log_n}] =
-        TuneVal{small ? 1 : 0, log_cols, 0.f};
+        TuneVal{small ? 1 : 0, log_cols, row_radix == 8 ? 3 : row_radix == 16 ? 4 : 0, 0.f};
     return BW_OK;
 }

@@ -76,6 +76,7 @@ struct bw_group_launch {
     uint32_t* d_err;    // bit 0: look-back wait timed out; bit 1: check failed
     int spin_limit;
     bool inject_wait_fault = false;  // test hook: every look-back wait runs out
+    int rlog = 0;       // row-pass radix log2 (0: radix 8 on the 64-bit path, 16 on the 32-bit)
 };
 int bw_enqueue_group(const bw_group_launch& g, cudaStream_t s);
 // Carry tiles of a group whose longest product has max_words output words.

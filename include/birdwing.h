@@ -390,16 +390,19 @@ int bw_batch_set_wait_limit(bw_batch* batch, int polls);
 int bw_batch_inject_wait_fault(bw_batch* batch, int enable);
 
 /* Time each candidate form of each group (one CTA per product where the
- * transform fits shared memory; 4-step with three column/row splits) on the
+ * transform fits shared memory; 4-step with each column/row split from
+ * square to long rows, each with row rounds of radix 8 and 16) on the
  * batch's own products, `reps` runs each, and keep the fastest in the
  * process-wide tune table that later layouts use.  Blocking. */
 int bw_batch_autotune(bw_batch* batch, int reps);
 /* The tune table as a JSON array of {path, num_primes, log_n, small,
- * log_cols, ms}.  Writes at most len bytes including the terminating NUL;
- * *needed gets the full size. */
+ * log_cols, row_radix, ms}.  Writes at most len bytes including the
+ * terminating NUL; *needed gets the full size. */
 int bw_tune_table_export(char* buf, size_t len, size_t* needed);
-/* Set one tune-table entry (log_cols 0 = automatic split). */
-int bw_tune_table_set(int path, int num_primes, int log_n, int small, int log_cols);
+/* Set one tune-table entry (log_cols 0 = automatic split; row_radix 8 or 16,
+ * or 0 for the path's default: 8 on the 64-bit path, 16 on the 32-bit). */
+int bw_tune_table_set(int path, int num_primes, int log_n, int small, int log_cols,
+                      int row_radix);
 
 /* ---------------------------------------------------------------- serving
  * A request loop with continuous batching.  Requests (host buffers) are

@@ -190,10 +190,35 @@ def test_autotune_and_tune_table_roundtrip():
         bt.run()
         for (p, a, b), got in zip(items, outs):
             assert (got == gmp_ref.mul(a, b)).all()
+    assert all(e["row_radix"] in (0, 8, 16) for e in table)
     bw.load_tune_table(table)
     # restore defaults for the other tests
     for p, ln in keys:
         bw.set_tune_entry(p, 2, ln, default_small(ln))
+
+
+@pytest.mark.parametrize("row_radix", [8, 16])
+def test_forced_row_radix_exact(row_radix):
+    # the 4-step groups with row rounds of either radix on both paths (the
+    # autotuner's candidates), rows from 2^6 to 2^12 points
+    rng = np.random.default_rng(13 + row_radix)
+    items = []
+    for p in (64, 32):
+        for words in (700, 3000, 20000, 60000):
+            items += [(p, rand_words(words, rng), rand_words(words // 3 + 1, rng))
+                      for _ in range(3)]
+    keys = {(p, log_n_of(p, len(a), len(b))) for p, a, b in items}
+    try:
+        for p, ln in keys:
+            bw.set_tune_entry(p, 2, ln, False, 0, row_radix)
+        with bw.Batch() as bt:
+            outs = [bt.add(a, b, path=p) for p, a, b in items]
+            bt.run()
+            for (p, a, b), got in zip(items, outs):
+                assert (got == gmp_ref.mul(a, b)).all(), (p, len(a), len(b), row_radix)
+    finally:
+        for p, ln in keys:
+            bw.set_tune_entry(p, 2, ln, default_small(ln))
 
 
 def test_uneven_mix_vs_gmp():
