@@ -150,8 +150,14 @@ struct TableBuilder {
     using T = typename Ar::T;
     std::vector<Tw<T>> host;
     // returns element offset of a new table
+    // every table starts at an even entry (16 bytes for 4-byte residues), so
+    // that the transforms can load its entries in pairs
+    void align_even() {
+        if (host.size() & 1) host.push_back(Tw<T>{0, 0});
+    }
     size_t add_stage_table(uint64_t p, uint64_t root, int log_len, int bits) {
         const size_t L = (size_t)1 << log_len;
+        align_even();
         const size_t off = host.size();
         host.resize(off + std::max<size_t>(L, 1));
         std::vector<uint64_t> pw(std::max<size_t>(L / 2, 1));
@@ -169,6 +175,7 @@ struct TableBuilder {
         return off;
     }
     size_t add_power_table(uint64_t p, uint64_t base, size_t count, uint64_t scale, int bits) {
+        align_even();
         const size_t off = host.size();
         host.resize(off + count);
         uint64_t w = scale % p;

@@ -225,6 +225,17 @@ __device__ __forceinline__ Tw<T> ld_w(const Tw<T>* p) {
     }
 }
 
+// Two consecutive twiddles (4-byte residues: one 16-byte load; the pair's
+// first entry has an even index in a 16-byte-aligned table).
+template <bool TS, typename T>
+__device__ __forceinline__ void ld_w2(const Tw<T>* p, Tw<T>& a, Tw<T>& b) {
+    static_assert(sizeof(T) == 4, "4-byte residues");
+    const uint4 v = TS ? *reinterpret_cast<const uint4*>(p)
+                       : __ldg(reinterpret_cast<const uint4*>(p));
+    a = Tw<T>{v.x, v.y};
+    b = Tw<T>{v.z, v.w};
+}
+
 // Forward CT stages s0 .. s0+RL-1 on one sub-problem of 2^RL elements that
 // belongs to group g of stage s0.  In the first round of a transform (s0 = 0)
 // stage 0 has twiddle 1 and inputs in [0, 2p), so its butterflies need no
@@ -249,6 +260,24 @@ __device__ __forceinline__ void ct_stages(typename Ar::T* x, int s0, int g,
             continue;
         }
         const Tw<T>* Ws = W + (1 << (s0 + l)) + (g << l);
+        if constexpr (sizeof(T) == 4) {
+            if (l > 0) {
+                // the level's 2^l twiddles in pairs
+#pragma unroll
+                for (int q = 0; q < (1 << l); q += 2) {
+                    Tw<T> w[2];
+                    ld_w2<TS>(Ws + q, w[0], w[1]);
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+#pragma unroll
+                        for (int u = 0; u < h; ++u) {
+                            const int k = ((q + e) << (RL - l)) + u;
+                            ar.ct(x[k], x[k + h], w[e].w, w[e].wq);
+                        }
+                }
+                continue;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < (1 << l); ++q) {
             const Tw<T> w = ld_w<TS>(Ws + q);
@@ -277,6 +306,23 @@ __device__ __forceinline__ void gs_stages(typename Ar::T* x, int s0, int g,
             continue;
         }
         const Tw<T>* Ws = W + (1 << (s0 + l)) + (g << l);
+        if constexpr (sizeof(T) == 4) {
+            if (l > 0) {
+#pragma unroll
+                for (int q = 0; q < (1 << l); q += 2) {
+                    Tw<T> w[2];
+                    ld_w2<TS>(Ws + q, w[0], w[1]);
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+#pragma unroll
+                        for (int u = 0; u < h; ++u) {
+                            const int k = ((q + e) << (RL - l)) + u;
+                            ar.gs(x[k], x[k + h], w[e].w, w[e].wq);
+                        }
+                }
+                continue;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < (1 << l); ++q) {
             const Tw<T> w = ld_w<TS>(Ws + q);
@@ -1368,18 +1414,30 @@ __device__ __forceinline__ void garner6_words_at(const PlanDev<Ar>& P,
             }
             k[i] = ai.red1(t);
         }
-        const uint64_t v4 = (uint64_t)k[5] * P.pr[4].ar.p + k[4];                  // < 2^60
-        const unsigned __int128 v3 = (unsigned __int128)v4 * P.pr[3].ar.p + k[3];  // < 2^90
-        const unsigned __int128 v2 = v3 * P.pr[2].ar.p + k[2];                     // < 2^120
-        // v2 p1 + k1 (< 2^150), then times p0 plus k0, in 64-bit words
-        const unsigned __int128 a0 = (unsigned __int128)(uint64_t)v2 * P.pr[1].ar.p + k[1];
-        const unsigned __int128 a1 =
-            (unsigned __int128)(uint64_t)(v2 >> 64) * P.pr[1].ar.p + (uint64_t)(a0 >> 64);
-        const uint64_t p0 = P.pr[0].ar.p;
-        const unsigned __int128 m0 = (unsigned __int128)(uint64_t)a0 * p0 + k[0];
-        const unsigned __int128 m1 = (unsigned __int128)(uint64_t)a1 * p0 + (uint64_t)(m0 >> 64);
-        const uint64_t c0 = (uint64_t)m0, c1 = (uint64_t)m1;
-        const uint64_t c2 = (uint64_t)(a1 >> 64) * p0 + (uint64_t)(m1 >> 64);
+        // Horner in 32-bit limbs, each step a chain of 32 x 32 + 64-bit
+        // multiply-adds: (k5 p4 + k4) (2 limbs), times p3 plus k3 (3), ...,
+        // times p0 plus k0 (6 limbs, < 2^178)
+        uint32_t w[6];
+        {
+            const uint64_t t = (uint64_t)k[5] * P.pr[4].ar.p + k[4];
+            w[0] = (uint32_t)t;
+            w[1] = (uint32_t)(t >> 32);
+        }
+#pragma unroll
+        for (int st = 0; st < 4; ++st) {
+            const uint32_t pm = P.pr[3 - st].ar.p;
+            uint64_t t = k[3 - st];
+#pragma unroll
+            for (int i = 0; i < 2 + st; ++i) {
+                t = (uint64_t)w[i] * pm + t;
+                w[i] = (uint32_t)t;
+                t >>= 32;
+            }
+            w[2 + st] = (uint32_t)t;
+        }
+        const uint64_t c0 = ((uint64_t)w[1] << 32) | w[0];
+        const uint64_t c1 = ((uint64_t)w[3] << 32) | w[2];
+        const uint64_t c2 = ((uint64_t)w[5] << 32) | w[4];
         bad |= (uint32_t)((c2 >> 32) != 0);
         const unsigned __int128 s0 = (unsigned __int128)acc0 + c0;
         l[2 * q] = (uint32_t)s0;
