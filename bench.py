@@ -1273,10 +1273,11 @@ def bench_plain(args):
     # the workload as the reference states it (its coefficient width and
     # prime count), when the library's own plan differs: same operands, same
     # timing, rank 0 of a single-GPU run
-    def side_record(which):
+    def side_record(which, e2e=False):
         """The same product under another plan of the table (same operands,
         same timing): the workload as the reference states it, or the other
-        prime path."""
+        prime path (e2e: also end to end from pinned host buffers, three
+        contexts in turn, as the headline's `e2e`)."""
         sp = plain_plan_args(cfg, which)
         with bw.Plan(*sp[:4], flags=sp[4]) as splan, bw.Context(splan) as sctx:
             sst = torch.cuda.ExternalStream(sctx.stream)
@@ -1289,11 +1290,41 @@ def bench_plain(args):
             sstage = stage_means(sctx, sst, 5)
             sctx.sync()
             si = splan.info
-            return {"algorithm": algorithm_of(si), "path": si["path"],
-                    "coeff_bits": si["coeff_bits"], "num_primes": si["num_primes"],
-                    "log_n": si["log_n"], "ms_per_step": sum(sper) / len(sper),
-                    "value": len(sper) / (sum(sper) * 1e-3), "unit": "products/s",
-                    "stage_ms": sstage, "correct_vs_gmp": sok, "_info": si}
+            rec = {"algorithm": algorithm_of(si), "path": si["path"],
+                   "coeff_bits": si["coeff_bits"], "num_primes": si["num_primes"],
+                   "log_n": si["log_n"], "ms_per_step": sum(sper) / len(sper),
+                   "value": len(sper) / (sum(sper) * 1e-3), "unit": "products/s",
+                   "stage_ms": sstage, "correct_vs_gmp": sok, "_info": si}
+            if e2e:
+                ring = [(sctx, hc)] + [
+                    (bw.Context(splan),
+                     torch.empty(la + lb, dtype=torch.int32).pin_memory().numpy().view(np.uint32))
+                    for _ in range(2)]
+                for c_, o_ in ring:
+                    c_.multiply_async(ha, hb, o_)
+                for c_, _ in ring:
+                    c_.sync()
+                steps = max(args.e2e_steps, 24)
+                t0 = time.perf_counter()
+                for i in range(steps):
+                    c_, o_ = ring[i % len(ring)]
+                    if i >= len(ring):
+                        c_.sync()
+                    c_.multiply_async(ha, hb, o_)
+                for c_, _ in ring:
+                    c_.sync()
+                dt = time.perf_counter() - t0
+                from oracle import gmp_ref
+                want = gmp_ref.mul(a, b)
+                rec["e2e"] = {"value": steps / dt, "unit": "products/s",
+                              "h2d_bytes_per_step": 4 * (la + (0 if square else lb)),
+                              "d2h_bytes_per_step": 4 * (la + lb),
+                              "correct_vs_gmp": all(bool((o_ == want).all()) for _, o_ in ring),
+                              "how": "bw_multiply(BW_PTR_HOST_ASYNC) on three contexts of one "
+                                     "plan in turn from pinned host buffers, wall clock"}
+                for c_, _ in ring[1:]:
+                    c_.close()
+            return rec
 
     literal = None
     if world == 1 and PLAIN[cfg]["literal"] != PLAIN[cfg]["plan"]:
@@ -1303,7 +1334,7 @@ def bench_plain(args):
     # coefficients for the 2^28-bit workloads)
     other = None
     if world == 1 and PLAIN[cfg].get("other"):
-        other = side_record("other")
+        other = side_record("other", e2e=cfg not in CPU_SAMPLE_WORDS)
 
     if rank == 0:
         ms = total_ms / args.steps
