@@ -35,6 +35,7 @@ struct Ar32 {
     uint32_t r32;   // 2^32 mod p
     uint32_t r32q;  // Shoup companion of r32
     uint32_t oneq;  // floor(2^32 / p): Shoup companion of 1
+    double pinv_d;  // 2^32 / p, for companions of twiddles built on the device
 
     __device__ __forceinline__ T red2(T a) const { return min(a, a - p2); }
     __device__ __forceinline__ T red1(T a) const { return min(a, a - p); }
@@ -80,9 +81,19 @@ struct Ar32 {
     __device__ __forceinline__ T inv_out(T a) const { return red1(a); }
     // x * w for a twiddle applied between transform passes, in [0, 2p)
     __device__ __forceinline__ T mulc(T x, T w, T wq) const { return shoup(x, w, wq); }
-    // Shoup companion floor(w 2^32 / p) of w < p
+    // Shoup companion floor(w 2^32 / p) of w < p: a double-precision estimate
+    // w (2^32 / p) is within 2^-20 of the quotient (below 2^32, relative error
+    // under 2^-51), so its floor is exact or one off, and the exact remainder
+    // w 2^32 - q p (in [-p, 2p)) decides the correction
     __device__ __forceinline__ T companion(T w) const {
-        return (uint32_t)((((uint64_t)w) << 32) / p);
+        uint32_t q = (uint32_t)((double)w * pinv_d);
+        const int64_t r = (int64_t)((((uint64_t)w) << 32) - (uint64_t)q * p);
+        if (r < 0) {
+            --q;
+        } else if (r >= (int64_t)p) {
+            ++q;
+        }
+        return q;
     }
     // a 64-bit coefficient x = h 2^32 + l reduced to [0, 2p): h (2^32 mod p)
     // and l * 1 by Shoup, each in [0, 2p), their sum below 4p

@@ -188,6 +188,7 @@ struct TableBuilder {
 };
 
 inline void set_c(Ar32& a, uint64_t p) {
+    a.pinv_d = 4294967296.0 / (double)p;
     a.r32 = (uint32_t)(((uint64_t)1 << 32) % p);
     a.r32q = (uint32_t)shoup_pre(a.r32, p, 32);
     a.oneq = (uint32_t)(((uint64_t)1 << 32) / p);
