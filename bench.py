@@ -1241,7 +1241,7 @@ def bench_plain(args):
     # still copies its operands in and its result out; the count covers the
     # pipeline's fill and drain.
     ring = [(ctx, hc)]
-    for _ in range(2 if n < (1 << 27) else 1):
+    for _ in range(3 if n < (1 << 27) else 1):
         ring.append((bw.Context(plan),
                      torch.empty(la + lb, dtype=torch.int32).pin_memory().numpy().view(np.uint32)))
     for c_, o_ in ring:
@@ -1276,7 +1276,7 @@ def bench_plain(args):
     def side_record(which, e2e=False):
         """The same product under another plan of the table (same operands,
         same timing): the workload as the reference states it, or the other
-        prime path (e2e: also end to end from pinned host buffers, three
+        prime path (e2e: also end to end from pinned host buffers, four
         contexts in turn, as the headline's `e2e`)."""
         sp = plain_plan_args(cfg, which)
         with bw.Plan(*sp[:4], flags=sp[4]) as splan, bw.Context(splan) as sctx:
@@ -1299,7 +1299,7 @@ def bench_plain(args):
                 ring = [(sctx, hc)] + [
                     (bw.Context(splan),
                      torch.empty(la + lb, dtype=torch.int32).pin_memory().numpy().view(np.uint32))
-                    for _ in range(2)]
+                    for _ in range(3)]
                 for c_, o_ in ring:
                     c_.multiply_async(ha, hb, o_)
                 for c_, _ in ring:
@@ -1320,7 +1320,7 @@ def bench_plain(args):
                               "h2d_bytes_per_step": 4 * (la + (0 if square else lb)),
                               "d2h_bytes_per_step": 4 * (la + lb),
                               "correct_vs_gmp": all(bool((o_ == want).all()) for _, o_ in ring),
-                              "how": "bw_multiply(BW_PTR_HOST_ASYNC) on three contexts of one "
+                              "how": "bw_multiply(BW_PTR_HOST_ASYNC) on four contexts of one "
                                      "plan in turn from pinned host buffers, wall clock"}
                 for c_, _ in ring[1:]:
                     c_.close()
@@ -1378,7 +1378,7 @@ def bench_plain(args):
             "e2e": {"value": job_throughput(e2e_steps, world, e2e_pipe_total),
                     "unit": "products/s", "h2d_bytes_per_step": 4 * (la + (0 if square else lb)),
                     "d2h_bytes_per_step": 4 * (la + lb) + 4,
-                    "how": "bw_multiply(BW_PTR_HOST_ASYNC) on three contexts of one plan in "
+                    "how": "bw_multiply(BW_PTR_HOST_ASYNC) on four contexts of one plan in "
                            "turn (stage-ordered copy-in / kernels / copy-out) from pinned host "
                            "buffers; wall clock over all steps with the pipeline's fill and "
                            "drain",
