@@ -82,3 +82,18 @@ def test_limb_conversions():
     assert w.dtype == np.uint32 and bw.limbs_to_int(w) == x
     assert bw.limbs_to_int(bw.int_to_limbs(7, 4)) == 7
     assert bw.limbs_to_int(np.array([1, 2], dtype=np.uint64)) == 1 + (2 << 64)
+
+
+def test_tune_table_entries():
+    # host-side table (no GPU): an entry with the row radix round-trips through
+    # the JSON export, and a radix other than 0, 8 or 16 is refused
+    bw.set_tune_entry(64, 2, 30, False, 15, 16)
+    bw.set_tune_entry(32, 2, 30, True)
+    table = {(e["path"], e["log_n"]): e for e in bw.tune_table()}
+    assert table[(64, 30)]["log_cols"] == 15 and table[(64, 30)]["row_radix"] == 16
+    assert table[(32, 30)]["small"] == 1 and table[(32, 30)]["row_radix"] == 0
+    with pytest.raises(bw.BwError) as e:
+        bw.set_tune_entry(64, 2, 30, False, 15, 32)
+    assert e.value.code == _lib.BW_EINVAL
+    bw.load_tune_table([table[(64, 30)]])
+    assert {(e["path"], e["log_n"]): e for e in bw.tune_table()}[(64, 30)]["row_radix"] == 16
